@@ -1,0 +1,158 @@
+/*
+ * symphas_b200.h -- C ABI of the B200 explicit finite-difference engine.
+ *
+ * This is the boundary between a host caller (the C++ MODEL/EVOLUTION front
+ * end in include/symphas_b200/, the Python package, or any FFI) and the
+ * sm_100a kernels.  Plain C types only; every call returns an int status
+ * (SP_OK = 0) and never throws; sp_last_error() gives the message of the last
+ * failure on a handle.
+ *
+ * What each entry point replaces in SymPhas (paths inside the SymPhas tree):
+ *
+ *   sp_create    Model<D,Sp,S...>(coeff, ncoeff, params) with
+ *                SolverFT<Stencil2d2h<L,G,B>|Stencil3d2h<L,G,B>>:
+ *                systems and dframe construction (sol/inc/model.h:100-128),
+ *                SolverFT::make_solver (examples/solvers/solverft.h:121-161),
+ *                StencilBase{2,3}d2h divh powers (sol/inc/stencilincludes.h:95-135)
+ *   sp_upload    writing the interior of system<i>().values
+ *                (sol/inc/solversystem.h:51-59) followed by update(t), the
+ *                halo refresh (datatypes/inc/boundaryupdate.h:154-356)
+ *   sp_step      n iterations of model_iteration: equation() then step(dt)
+ *                then update(t) (modules-models.h:435-467;
+ *                examples/solvers/solverft.h:46-50, :90-103)
+ *   sp_download  reading the interior of system<i>().values / get_field<i>()
+ *   sp_reduce    the density and energy collectors evaluated at save points
+ *                (dataprocesses/datadensity.h, dataprocesses/dataenergy.h)
+ *   sp_destroy   ~Model
+ *
+ * Threading: a handle is used by one host thread at a time; all its work runs
+ * in order on one CUDA stream (its own, or the one given by sp_set_stream).
+ * Ownership: the handle owns its device buffers; the caller owns host buffers.
+ */
+#ifndef SYMPHAS_B200_H
+#define SYMPHAS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SP_OK 0
+#define SP_EINVAL 1      /* bad argument or unsupported combination */
+#define SP_ECUDA 2       /* a CUDA runtime call failed */
+#define SP_ENOMEM 3      /* device allocation failed */
+#define SP_ETIMEOUT 4    /* a bounded device wait gave up (error flag set by a kernel) */
+#define SP_ENONFINITE 5  /* a reduction saw NaN or Inf */
+
+/* dtype of the fields on the device */
+#define SP_F32 0
+#define SP_F64 1
+
+/* boundary kind of one side (order LEFT RIGHT TOP BOTTOM FRONT BACK, i.e.
+ * x-, x+, y-, y+, z-, z+ as in Side, lib/inc/definitions.h:588) */
+#define SP_PERIODIC 0
+#define SP_DIRICHLET 1 /* BoundaryType::DEFAULT with BoundaryTag::CONSTANT */
+
+/* built-in models (each lowered at build time into fused kernels) */
+#define SP_MODEL_A 0      /* MA:  dpsi = lap(psi) + (c1 - c2 psi^2) psi                */
+#define SP_MODEL_B 1      /* MB:  dpsi = -bilap(psi) - lap((c1 - c2 psi^2) psi)        */
+#define SP_MODEL_C 2      /* two fields psi, eta; gamma = c1:
+                             dpsi = lap(-psi + psi^3 + 2 gamma psi eta^2 - lap psi)
+                             deta = eta - eta^3 - 2 gamma psi^2 eta + lap eta          */
+#define SP_MODEL_AMK 3    /* dpsi = M (kappa lap psi - psi^3 + psi), M = c1, kappa = c2 */
+#define SP_MODEL_BMK 4    /* dpsi = M lap(psi^3 - psi - kappa lap psi)                  */
+#define SP_OP_LAP 10      /* dframe = lap(psi)       (single-operator models used to   */
+#define SP_OP_BILAP 11    /* dframe = bilap(psi)      check every stencil point set)    */
+#define SP_OP_GRADLAP 12  /* dframe = x component of gradlap(psi)                       */
+#define SP_OP_LAPCUBE 13  /* dframe = lap(psi^3)                                        */
+
+/* evaluation form */
+#define SP_FORM_EXACT 1 /* the printed scheme of SymPhas, term by term, no FMA
+                           contraction: bit-identical to the CPU solver in FP64 */
+#define SP_FORM_FUSED 0 /* algebraically equal fused form (bilap = lap o lap,
+                           derivatives of a sum merged, staged in shared memory) */
+
+typedef struct sp_desc {
+  int dim;              /* 2 or 3 */
+  int n[3];             /* interior extents x, y, z (z ignored when dim == 2) */
+  int dtype;            /* SP_F32 or SP_F64 */
+  int model;            /* SP_MODEL_* or SP_OP_* */
+  int form;             /* SP_FORM_EXACT or SP_FORM_FUSED */
+  int lap_pts;          /* Stencil2d2h<L,G,B> / Stencil3d2h<L,G,B> point counts */
+  int gradlap_pts;
+  int bilap_pts;
+  int boundary[6];      /* SP_PERIODIC or SP_DIRICHLET per side */
+  double boundary_value[6];
+  double h;             /* uniform grid spacing */
+  double dt;            /* forward-Euler time step */
+  double coeff[8];      /* c(1)..c(8); unused entries should be 1 (c(i) default) */
+  int ncoeff;
+  int batch;            /* number of identical independent instances (>= 1) */
+} sp_desc;
+
+typedef struct sp_handle sp_handle;
+
+/* Create a handle: validates the description, allocates the device fields
+ * (interior + halo, ping-pong) and builds the TMA descriptors. */
+int sp_create(const sp_desc* desc, sp_handle** out);
+
+/* Copy `bytes` of interior values (x-fastest, dtype of the handle) of field
+ * `field` of instance `inst` from host memory, then refresh its halo. */
+int sp_upload(sp_handle* h, int inst, int field, const void* host, size_t bytes);
+/* Same from device memory (bytes in the same compact interior layout). */
+int sp_upload_device(sp_handle* h, int inst, int field, const void* dev, size_t bytes);
+/* Fill field `field` of instance `inst` with the seeded SplitMix64 stream
+ * value(i) = lo + (hi - lo) * u53(seed, i), bit-identical to the oracle. */
+int sp_fill_uniform(sp_handle* h, int inst, int field, uint64_t seed, double lo, double hi);
+
+/* Advance every instance by `nsteps` forward-Euler iterations. */
+int sp_step(sp_handle* h, int nsteps);
+
+/* Advance every instance by `nsteps` (>= 1) iterations; the last one also sums
+ * field 0 of each instance in FP64 inside the step kernel (warp shuffles) and
+ * writes the `batch` sums to `mass`.  Waits for the result. */
+int sp_step_mass(sp_handle* h, int nsteps, double* mass);
+
+/* Evaluate the right-hand side (dframe) of the current state once, without
+ * stepping, and copy field `field` of instance `inst` to host memory. */
+int sp_eval_rhs(sp_handle* h, int inst, int field, void* host, size_t bytes);
+
+/* Copy the interior of field `field` of instance `inst` to host memory and
+ * wait for the copy. */
+int sp_download(sp_handle* h, int inst, int field, void* host, size_t bytes);
+/* Same into device memory (compact interior layout), stream-ordered. */
+int sp_download_device(sp_handle* h, int inst, int field, void* dev, size_t bytes);
+
+/* FP64 reductions over the interior of field `field` of instance `inst`:
+ * mass = sum of values, energy = h^D * sum of the model's free-energy density
+ * (forward-difference gradients).  Waits for the result. */
+int sp_reduce(sp_handle* h, int inst, int field, double* mass, double* energy);
+
+/* Change the time step of further sp_step calls (SolverFT's dt, set by
+ * Model::step at sol/inc/model.h:932-936). */
+int sp_set_dt(sp_handle* h, double dt);
+
+/* Run all further work of the handle on `stream` (a cudaStream_t). */
+int sp_set_stream(sp_handle* h, void* stream);
+/* Wait until all queued work of the handle is done. */
+int sp_synchronize(sp_handle* h);
+/* Number of fused-step kernel launches issued so far by this handle. */
+long long sp_launch_count(const sp_handle* h);
+/* Device pointer of the current interior origin of a field and its
+ * padded geometry (pitch and halo in elements), for zero-copy callers. */
+int sp_field_geometry(const sp_handle* h, int inst, int field, void** dev_origin,
+                      long long* pitch, long long* plane, int halo[3]);
+
+const char* sp_last_error(const sp_handle* h);
+/* Message of the last failure of sp_create (no handle exists then). */
+const char* sp_create_error(void);
+void sp_destroy(sp_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SYMPHAS_B200_H */

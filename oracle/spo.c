@@ -1,0 +1,646 @@
+/*
+ * spo.c -- CPU oracle for the explicit finite-difference path of SymPhas.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product (the symphas_b200
+ * package, its CUDA library or the C++ front end) may include, link or run
+ * this file; only tests/, the smoke check and the CPU-baseline leg of
+ * bench.py use it, and only as the checker.
+ *
+ * What it restates (paths are inside the SymPhas source tree):
+ *   - storage: x-fastest, BOUNDARY_DEPTH = 3 halo cells on every side
+ *     (datatypes/inc/gridinfo.h:46, grid::get_stride datatypes/inc/grid.h:536-580)
+ *   - halo refresh before every evaluation: periodic copies of the opposite
+ *     interior (datatypes/inc/boundaryupdate.h:154-356, :650-690) and the
+ *     constant DEFAULT/CONSTANT boundary (datatypes/inc/boundaryupdate.h:1148-1526)
+ *   - stencils of 2nd-order accuracy, every point variant, with their
+ *     summation order (sol/inc/stencilh2.h:87-507) and the divh powers
+ *     divh2 = divh*divh, divh3 = divh*divh2, divh4 = divh2*divh2
+ *     (sol/inc/stencilincludes.h:100-107)
+ *   - derivatives of non-variable expressions are materialised first over the
+ *     whole storage, halo included, then the stencil runs on the temporary
+ *     (sym/inc/expressionderivatives.h:1546-1588)
+ *   - sums of terms are a right fold e0 + (e1 + (e2 + ...))
+ *     (sym/inc/expressions.h:2032-2040); power<N> for N <= 6 is the right-fold
+ *     product x*(x*x) (lib/inc/spslibmath.h:255-268)
+ *   - equations of all fields are evaluated before any field is stepped
+ *     (sol/inc/modelspecialized.h:377-385, sol/inc/model.h:932-936), and the
+ *     step is psi + dt*dframe over the interior (examples/solvers/solverft.h:46-50)
+ *
+ * Parity status: the SymPhas CPU solver could not be built here (its headers
+ * need CMake-generated configuration files and two source patches for GCC 13),
+ * so this restatement is pinned by known-answer tests (analytic stencil
+ * results, the manufactured-solution convergence example of SymPhas,
+ * conservation) rather than by outputs of SymPhas itself: parity unpinned.
+ *
+ * Build: oracle/Makefile (gcc -O2 -ffp-contract=off -fopenmp -shared).
+ * Floating-point contraction is disabled so every product and sum rounds on
+ * its own, as in the reference's plain C++ expression evaluation.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define BD 3 /* BOUNDARY_DEPTH */
+
+enum {
+  SPO_MODEL_A = 0,      /* dpsi = lap(psi) + (c1 - c2 psi^2) psi          */
+  SPO_MODEL_B = 1,      /* dpsi = -bilap(psi) - lap((c1 - c2 psi^2) psi)  */
+  SPO_MODEL_C = 2,      /* two fields, coupling 2*gamma*psi*eta^2         */
+  SPO_MODEL_AMK = 3,    /* dpsi = M (kappa lap psi - psi^3 + psi)         */
+  SPO_MODEL_BMK = 4,    /* dpsi = M lap(psi^3 - psi - kappa lap psi)      */
+  SPO_OP_LAP = 10,      /* dframe = lap(psi)         (operator checks)    */
+  SPO_OP_BILAP = 11,    /* dframe = bilap(psi)                            */
+  SPO_OP_GRADLAP = 12,  /* dframe = x-component of gradlap(psi)           */
+  SPO_OP_LAPCUBE = 13,  /* dframe = lap(psi^3)                            */
+};
+
+enum { SPO_PERIODIC = 0, SPO_DIRICHLET = 1 };
+
+typedef struct spo_desc {
+  int dim;          /* 2 or 3 */
+  int n[3];         /* interior extents x, y, z (z ignored in 2D) */
+  int model;
+  int lap_pts, gradlap_pts, bilap_pts;
+  double h, dt;
+  double c[8];      /* c(1)..c(8) */
+  int bc[6];        /* sides in the order LEFT RIGHT TOP BOTTOM FRONT BACK */
+  double bcv[6];    /* constant value of a DIRICHLET side */
+} spo_desc;
+
+/* ------------------------------------------------------------------ */
+/* seeded initial values: SplitMix64 counter stream                    */
+/* ------------------------------------------------------------------ */
+
+static uint64_t spo_mix(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+/* value i of stream `seed`: lo + (hi - lo) * u, u = top 53 bits / 2^53 */
+void spo_seed_uniform(uint64_t seed, double lo, double hi, long long count,
+                      long long first, double* out) {
+  const double inv = 1.0 / 9007199254740992.0; /* 2^-53 */
+  for (long long i = 0; i < count; ++i) {
+    uint64_t z = seed + (uint64_t)(first + i + 1) * 0x9E3779B97F4A7C15ULL;
+    double u = (double)(spo_mix(z) >> 11) * inv;
+    out[i] = lo + (hi - lo) * u;
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* grids                                                               */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+  int dim;
+  long L[3];      /* storage extents incl. halo */
+  long s[3];      /* strides {1, Lx, Lx*Ly} */
+  long size;
+} spo_geom;
+
+static spo_geom spo_make_geom(const spo_desc* d) {
+  spo_geom g;
+  g.dim = d->dim;
+  g.L[0] = d->n[0] + 2 * BD;
+  g.L[1] = d->n[1] + 2 * BD;
+  g.L[2] = (d->dim == 3) ? d->n[2] + 2 * BD : 1;
+  g.s[0] = 1;
+  g.s[1] = g.L[0];
+  g.s[2] = g.L[0] * g.L[1];
+  g.size = g.L[0] * g.L[1] * g.L[2];
+  return g;
+}
+
+/* Fill the halo.  A halo cell outside the domain along a DIRICHLET axis takes
+ * that side's value (later sides in LEFT..BACK order win); a cell outside only
+ * along periodic axes takes the value of its periodic image. */
+static void spo_update_halo(const spo_desc* d, const spo_geom* g, double* v) {
+  const int D = d->dim;
+  const long kz0 = (D == 3) ? 0 : 0, kz1 = g->L[2];
+  for (long k = kz0; k < kz1; ++k)
+    for (long j = 0; j < g->L[1]; ++j)
+      for (long i = 0; i < g->L[0]; ++i) {
+        long c[3] = {i - BD, j - BD, (D == 3) ? k - BD : 0};
+        int outside = 0;
+        for (int a = 0; a < D; ++a)
+          if (c[a] < 0 || c[a] >= d->n[a]) outside = 1;
+        if (!outside) continue;
+        int dir = -1;
+        double dval = 0;
+        for (int a = 0; a < D; ++a) {
+          if (c[a] < 0 && d->bc[2 * a] == SPO_DIRICHLET) { dir = 2 * a; dval = d->bcv[2 * a]; }
+          if (c[a] >= d->n[a] && d->bc[2 * a + 1] == SPO_DIRICHLET) { dir = 2 * a + 1; dval = d->bcv[2 * a + 1]; }
+        }
+        long idx = i + j * g->s[1] + k * g->s[2];
+        if (dir >= 0) {
+          v[idx] = dval;
+          continue;
+        }
+        long w[3];
+        for (int a = 0; a < 3; ++a) {
+          long n = (a < D) ? d->n[a] : 1;
+          long x = c[a];
+          if (a < D) {
+            while (x < 0) x += n;
+            while (x >= n) x -= n;
+          }
+          w[a] = x + ((a < D) ? BD : 0);
+        }
+        v[idx] = v[w[0] + w[1] * g->s[1] + w[2] * g->s[2]];
+      }
+}
+
+/* ------------------------------------------------------------------ */
+/* stencils (sol/inc/stencilh2.h), neighbour names as in sol/inc/stencil.h */
+/* ------------------------------------------------------------------ */
+
+#define P(i, j, k) v[(i) * sx + (j) * sy + (k) * sz]
+#define v0 P(0, 0, 0)
+#define vx P(1, 0, 0)
+#define vx_ P(-1, 0, 0)
+#define vy P(0, 1, 0)
+#define vy_ P(0, -1, 0)
+#define vz P(0, 0, 1)
+#define vz_ P(0, 0, -1)
+#define vx2 P(2, 0, 0)
+#define vx2_ P(-2, 0, 0)
+#define vy2 P(0, 2, 0)
+#define vy2_ P(0, -2, 0)
+#define vz2 P(0, 0, 2)
+#define vz2_ P(0, 0, -2)
+#define vxy P(1, 1, 0)
+#define vxy_ P(1, -1, 0)
+#define vx_y P(-1, 1, 0)
+#define vx_y_ P(-1, -1, 0)
+#define vx2y P(2, 1, 0)
+#define vx2y_ P(2, -1, 0)
+#define vx2_y P(-2, 1, 0)
+#define vx2_y_ P(-2, -1, 0)
+#define vxy2 P(1, 2, 0)
+#define vxy2_ P(1, -2, 0)
+#define vx_y2 P(-1, 2, 0)
+#define vx_y2_ P(-1, -2, 0)
+#define vx2y2 P(2, 2, 0)
+#define vx2y2_ P(2, -2, 0)
+#define vx2_y2 P(-2, 2, 0)
+#define vx2_y2_ P(-2, -2, 0)
+#define vxz P(1, 0, 1)
+#define vxz_ P(1, 0, -1)
+#define vx_z P(-1, 0, 1)
+#define vx_z_ P(-1, 0, -1)
+#define vx2z P(2, 0, 1)
+#define vx2z_ P(2, 0, -1)
+#define vx2_z P(-2, 0, 1)
+#define vx2_z_ P(-2, 0, -1)
+#define vxz2 P(1, 0, 2)
+#define vxz2_ P(1, 0, -2)
+#define vx_z2 P(-1, 0, 2)
+#define vx_z2_ P(-1, 0, -2)
+#define vx2z2 P(2, 0, 2)
+#define vx2z2_ P(2, 0, -2)
+#define vx2_z2 P(-2, 0, 2)
+#define vx2_z2_ P(-2, 0, -2)
+#define vyz P(0, 1, 1)
+#define vyz_ P(0, 1, -1)
+#define vy_z P(0, -1, 1)
+#define vy_z_ P(0, -1, -1)
+#define vyz2 P(0, 1, 2)
+#define vyz2_ P(0, 1, -2)
+#define vy_z2 P(0, -1, 2)
+#define vy_z2_ P(0, -1, -2)
+#define vy2z P(0, 2, 1)
+#define vy2z_ P(0, 2, -1)
+#define vy2_z P(0, -2, 1)
+#define vy2_z_ P(0, -2, -1)
+#define vy2z2 P(0, 2, 2)
+#define vy2z2_ P(0, 2, -2)
+#define vy2_z2 P(0, -2, 2)
+#define vy2_z2_ P(0, -2, -2)
+#define vxyz P(1, 1, 1)
+#define vxyz_ P(1, 1, -1)
+#define vxy_z P(1, -1, 1)
+#define vxy_z_ P(1, -1, -1)
+#define vx_yz P(-1, 1, 1)
+#define vx_yz_ P(-1, 1, -1)
+#define vx_y_z P(-1, -1, 1)
+#define vx_y_z_ P(-1, -1, -1)
+#define vx2yz P(2, 1, 1)
+#define vx2yz_ P(2, 1, -1)
+#define vx2y_z P(2, -1, 1)
+#define vx2y_z_ P(2, -1, -1)
+#define vx2_yz P(-2, 1, 1)
+#define vx2_yz_ P(-2, 1, -1)
+#define vx2_y_z P(-2, -1, 1)
+#define vx2_y_z_ P(-2, -1, -1)
+#define vxy2z P(1, 2, 1)
+#define vxy2z_ P(1, 2, -1)
+#define vxy2_z P(1, -2, 1)
+#define vxy2_z_ P(1, -2, -1)
+#define vx_y2z P(-1, 2, 1)
+#define vx_y2z_ P(-1, 2, -1)
+#define vx_y2_z P(-1, -2, 1)
+#define vx_y2_z_ P(-1, -2, -1)
+#define vxyz2 P(1, 1, 2)
+#define vxyz2_ P(1, 1, -2)
+#define vxy_z2 P(1, -1, 2)
+#define vxy_z2_ P(1, -1, -2)
+#define vx_yz2 P(-1, 1, 2)
+#define vx_yz2_ P(-1, 1, -2)
+#define vx_y_z2 P(-1, -1, 2)
+#define vx_y_z2_ P(-1, -1, -2)
+#define vx2y2z2 P(2, 2, 2)
+#define vx2y2z2_ P(2, 2, -2)
+#define vx2y2_z2 P(2, -2, 2)
+#define vx2y2_z2_ P(2, -2, -2)
+#define vx2_y2z2 P(-2, 2, 2)
+#define vx2_y2z2_ P(-2, 2, -2)
+#define vx2_y2_z2 P(-2, -2, 2)
+#define vx2_y2_z2_ P(-2, -2, -2)
+
+typedef struct {
+  long sx, sy, sz;
+  double divh2, divh3, divh4;
+  int lap, grad, bilap, dim;
+} spo_stencil;
+
+/* sol/inc/stencilh2.h:87-107 (2D) and :235-327 (3D) */
+static double spo_lap(const spo_stencil* st, const double* v) {
+  const long sx = st->sx, sy = st->sy, sz = st->sz;
+  const double divh2 = st->divh2;
+  if (st->dim == 2) {
+    switch (st->lap) {
+      case 5: return (vx_ + vx + vy + vy_ - 4. * v0) * divh2;
+      case 9:
+        return (vx_y + vxy_ + vxy + vx_y_ + 4. * vx + 4. * vy + 4. * vy_ + 4. * vx_ - 20. * v0) *
+               divh2 * (1.0 / 6);
+    }
+  } else {
+    switch (st->lap) {
+      case 7: return (vx_ + vx + vy + vy_ + vz + vz_ - 6. * v0) * divh2;
+      case 15:
+        return (vx_y_z_ + vxy_z_ + vx_yz_ + vxyz_ + vx_y_z + vxy_z + vx_yz + vxyz +
+                8. * (vx_ + vx + vy + vy_ + vz + vz_ - 7. * v0)) *
+               divh2 * (1.0 / 12);
+      case 19: /* the reference reads vz twice here (stencilh2.h:273) */
+        return (vx_y_ + vxy_ + vx_y + vxy + vx_z_ + vxz_ + vx_z + vxz + vy_z_ + vyz_ + vy_z +
+                vyz + 2. * (vx_ + vx + vy + vy_ + vz + vz) - 24. * v0) *
+               divh2 * (1.0 / 6);
+      case 21:
+        return (-(vx_y_z_ + vxy_z_ + vx_yz_ + vxyz_ + vx_y_z + vxy_z + vx_yz + vxyz) +
+                4. * (vx_y_ + vxy_ + vx_y + vxy + vx_z_ + vxz_ + vx_z + vxz + vy_z_ + vyz_ +
+                      vy_z + vyz) +
+                -40. * v0) *
+               divh2 * (1.0 / 12);
+      case 27:
+        return (vx_y_z_ + vxy_z_ + vx_yz_ + vxyz_ + vx_y_z + vxy_z + vx_yz + vxyz +
+                3. * (vx_y_ + vxy_ + vx_y + vxy + vx_z_ + vxz_ + vx_z + vxz + vy_z_ + vyz_ +
+                      vy_z + vyz) +
+                14. * (vx_ + vx + vy + vy_ + vz + vz_) - 128. * v0) *
+               divh2 * (1.0 / 30);
+    }
+  }
+  abort();
+}
+
+/* sol/inc/stencilh2.h:112-156 (2D) and :329-412 (3D) */
+static double spo_bilap(const spo_stencil* st, const double* v) {
+  const long sx = st->sx, sy = st->sy, sz = st->sz;
+  const double divh4 = st->divh4;
+  if (st->dim == 2) {
+    switch (st->bilap) {
+      case 13:
+        return (vy2_ + vy2 + vx2_ + vx2 + 2. * (vx_y_ + vxy_ + vx_y + vxy) -
+                8. * (vx_ + vx + vy_ + vy) + 20. * v0) *
+               divh4;
+      case 17:
+        return ((vx2y2 + vx2_y2 + vx2y2_ + vx2_y2_) + 10. * (vx2 + vx2_ + vy2 + vy2_) +
+                8. * (vxy + vx_y + vxy_ + vx_y_) - 64. * (vx + vx_ + vy + vy_) + 180. * v0) *
+               divh4 * (1.0 / 12);
+      case 21:
+        return ((vx2y + vx2_y + vx2y_ + vx2_y_ + vxy2 + vx_y2 + vxy2_ + vx_y2_) +
+                (vx2 + vx2_ + vy2 + vy2_) - 2. * (vxy + vx_y + vxy_ + vx_y_) -
+                10. * (vx + vx_ + vy + vy_) + 36. * v0) *
+               divh4 * (1.0 / 12);
+    }
+  } else {
+    switch (st->bilap) {
+      case 21:
+        return ((vx2y2 + vx2_y2 + vx2y2_ + vx2_y2_ + vx2z2_ + vx2_z2_ + vx2z2 + vx2_z2 + vy2z2_ +
+                 vy2z2 + vy2_z2_ + vy2_z2) -
+                4. * (vxyz + vx_yz + vxy_z + vx_y_z + vxyz_ + vx_yz_ + vxy_z_ + vx_y_z_) +
+                20. * v0) *
+               divh4 * (1.0 / 4);
+      case 25:
+        return (2. * (vxy + vx_y + vxy_ + vx_y_ + vxz_ + vx_z_ + vxz + vx_z + vyz_ + vyz +
+                      vy_z_ + vy_z) +
+                (vx2 + vx2_ + vy2 + vy2_ + vz2 + vz2_) -
+                12. * (vx + vx_ + vy + vy_ + vz + vz_) + 42. * v0) *
+               divh4;
+      case 41:
+        return ((vx2y2z2 + vx2_y2z2 + vx2y2_z2 + vx2_y2_z2 + vx2y2z2_ + vx2_y2z2_ + vx2y2_z2_ +
+                 vx2_y2_z2_) -
+                40. * (vxyz + vx_yz + vxy_z + vx_y_z + vxyz_ + vx_yz_ + vxy_z_ + vx_y_z_) +
+                96. * (vxy + vx_y + vxy_ + vx_y_ + vxz_ + vx_z_ + vxz + vx_z + vyz_ + vyz +
+                       vy_z_ + vy_z) +
+                20. * (vx2 + vx2_ + vy2 + vy2_ + vz2 + vz2_) -
+                320. * (vx + vx_ + vy + vy_ + vz + vz_) + 960. * v0) *
+               divh4 * (1.0 / 24);
+      case 52:
+        return (-(vx2y2z2 + vx2_y2z2 + vx2y2_z2 + vx2_y2_z2 + vx2y2z2_ + vx2_y2z2_ + vx2y2_z2_ +
+                  vx2_y2_z2_) +
+                10. * (vxyz2 + vx_yz2 + vxy_z2 + vx_y_z2 + vxyz2_ + vx_yz2_ + vxy_z2_ +
+                       vx_y_z2_ + vxy2z + vx_y2z + vxy2_z + vx_y2_z + vxy2z_ + vx_y2z_ +
+                       vxy2_z_ + vx_y2_z_ + vx2yz + vx2_yz + vx2y_z + vx2_y_z + vx2yz_ +
+                       vx2_yz_ + vx2y_z_ + vx2_y_z_) -
+                20. * (vxyz + vx_yz + vxy_z + vx_y_z + vxyz_ + vx_yz_ + vxy_z_ + vx_y_z_) -
+                36. * (vxy + vx_y + vxy_ + vx_y_ + vxz_ + vx_z_ + vxz + vx_z + vyz_ + vyz +
+                       vy_z_ + vy_z) +
+                360. * v0) *
+               divh4 * (1.0 / 36);
+      case 57:
+        return ((vyz2 + vy_z2 + vyz2_ + vy_z2_ + vy2z + vy2_z + vy2z_ + vy2_z_ + vx2z + vx2_z +
+                 vx2z_ + vx2_z_ + vxz2 + vx_z2 + vxz2_ + vx_z2_ + vxy2 + vx_y2 + vxy2_ +
+                 vx_y2_ + vx2y + vx2_y + vx2y_ + vx2_y_) +
+                3. * (vxyz + vx_yz + vxy_z + vx_y_z + vxyz_ + vx_yz_ + vxy_z_ + vx_y_z_) -
+                8. * (vxy + vx_y + vxy_ + vx_y_ + vxz_ + vx_z_ + vxz + vx_z + vyz_ + vyz +
+                      vy_z_ + vy_z) -
+                (vx2 + vx2_ + vy2 + vy2_ + vz2 + vz2_) +
+                4. * (vx + vx_ + vy + vy_ + vz + vz_) + 30. * v0) *
+               divh4 * (1.0 / 3);
+    }
+  }
+  abort();
+}
+
+/* x component of the gradlaplacian, sol/inc/stencilh2.h:161-221, :417-507 */
+static double spo_gradlap_x(const spo_stencil* st, const double* v) {
+  const long sx = st->sx, sy = st->sy, sz = st->sz;
+  const double divh3 = st->divh3;
+  if (st->dim == 2) {
+    switch (st->grad) {
+      case 6:
+        return ((vx2y - vx2_y + vx2y_ - vx2_y_) - 4. * (vx - vx_)) * divh3 * (1.0 / 4);
+      case 8:
+        return ((vx2 - vx2_) + (vxy - vx_y + vxy_ - vx_y_) - 4. * (vx - vx_)) * divh3 *
+               (1.0 / 2);
+      case 12:
+        return ((vx2y2 - vx2_y2 + vx2y2_ - vx2_y2_) + 10. * (vx2 - vx2_) +
+                4. * (vxy - vx_y + vxy_ - vx_y_) - 32. * (vx - vx_)) *
+               divh3 * (1.0 / 24);
+      case 16:
+        return (2. * (vx2y - vx2_y + vx2y_ - vx2_y_) + 2. * (vx2 - vx2_) +
+                (vxy2 - vx_y2 + vxy2_ - vx_y2_) - 2. * (vxy - vx_y + vxy_ - vx_y_) -
+                10. * (vx - vx_)) *
+               divh3 * (1.0 / 12);
+    }
+  } else {
+    switch (st->grad) {
+      case 10:
+        return ((vx2yz - vx2_yz + vx2y_z - vx2_y_z + vx2yz_ - vx2_yz_ + vx2y_z_ - vx2_y_z_) -
+                8. * (vx - vx_)) *
+               divh3 * (1.0 / 8);
+      case 12:
+        return ((vx2 - vx2_) + (vxy - vx_y + vxy_ - vx_y_ + vxz_ - vx_z_ + vxz - vx_z) -
+                6. * (vx - vx_)) *
+               divh3 * (1.0 / 2);
+      case 28:
+        return ((vx2y2 - vx2_y2 + vx2y2_ - vx2_y2_ + vx2z2_ - vx2_z2_ + vx2z2 - vx2_z2) +
+                8. * (vx2 - vx2_) +
+                6. * (vxyz - vx_yz + vxy_z - vx_y_z + vxyz_ - vx_yz_ + vxy_z_ - vx_y_z_) -
+                8. * (vxy - vx_y + vxy_ - vx_y_ + vxz_ - vx_z_ + vxz - vx_z) -
+                16. * (vx - vx_)) *
+               divh3 * (1.0 / 24);
+      case 36:
+        return (2. * (vx2z - vx2_z + vx2z_ - vx2_z_ + vx2y - vx2_y + vx2y_ - vx2_y_) -
+                2. * (vx2 - vx2_) +
+                (vxz2 - vx_z2 + vxz2_ - vx_z2_ + vxy2 - vx_y2 + vxy2_ - vx_y2_) +
+                3. * (vxyz - vx_yz + vxy_z - vx_y_z + vxyz_ - vx_yz_ + vxy_z_ - vx_y_z_) -
+                8. * (vxy - vx_y + vxy_ - vx_y_ + vxz_ - vx_z_ + vxz - vx_z) +
+                4. * (vx - vx_)) *
+               divh3 * (1.0 / 12);
+      case 40:
+        return (16. * (vx2z - vx2_z + vx2z_ - vx2_z_ + vx2y - vx2_y + vx2y_ - vx2_y_) -
+                16. * (vx2 - vx2_) +
+                3. * (vxy2z - vx_y2z + vxy2_z - vx_y2_z + vxy2z_ - vx_y2z_ + vxy2_z_ -
+                      vx_y2_z_ + vxyz2 - vx_yz2 + vxy_z2 - vx_y_z2 + vxyz2_ - vx_yz2_ +
+                      vxy_z2_ - vx_y_z2_) +
+                2. * (vxz2 - vx_z2 + vxz2_ - vx_z2_ + vxy2 - vx_y2 + vxy2_ - vx_y2_) -
+                22. * (vxy - vx_y + vxy_ - vx_y_ + vxz_ - vx_z_ + vxz - vx_z) -
+                40. * (vx - vx_)) *
+               divh3 * (1.0 / 96);
+    }
+  }
+  abort();
+}
+
+/* ------------------------------------------------------------------ */
+/* models                                                              */
+/* ------------------------------------------------------------------ */
+
+static int spo_field_count(int model) { return model == SPO_MODEL_C ? 2 : 1; }
+
+static double pow3(double x) { return x * (x * x); }
+
+typedef struct {
+  spo_desc d;
+  spo_geom g;
+  spo_stencil st;
+  int nf;
+  double* psi[2];    /* storage incl. halo */
+  double* dframe[2];
+  double* tmp[2];    /* materialised operands of derivatives */
+  int threads;
+} spo_sys;
+
+static void spo_sys_init(spo_sys* s, const spo_desc* d, int threads) {
+  memset(s, 0, sizeof(*s));
+  s->d = *d;
+  s->g = spo_make_geom(d);
+  s->nf = spo_field_count(d->model);
+  s->threads = threads > 0 ? threads : 1;
+  double divh = 1.0 / d->h;
+  s->st.divh2 = divh * divh;
+  s->st.divh3 = divh * s->st.divh2;
+  s->st.divh4 = s->st.divh2 * s->st.divh2;
+  s->st.sx = 1;
+  s->st.sy = s->g.s[1];
+  s->st.sz = (d->dim == 3) ? s->g.s[2] : 0;
+  s->st.lap = d->lap_pts;
+  s->st.grad = d->gradlap_pts;
+  s->st.bilap = d->bilap_pts;
+  s->st.dim = d->dim;
+  for (int f = 0; f < 2; ++f) {
+    s->psi[f] = (double*)calloc(s->g.size, sizeof(double));
+    s->dframe[f] = (double*)calloc(s->g.size, sizeof(double));
+    s->tmp[f] = (double*)calloc(s->g.size, sizeof(double));
+  }
+}
+
+static void spo_sys_free(spo_sys* s) {
+  for (int f = 0; f < 2; ++f) {
+    free(s->psi[f]);
+    free(s->dframe[f]);
+    free(s->tmp[f]);
+  }
+}
+
+#define SPO_FOR_STORAGE(body)                                   \
+  _Pragma("omp parallel for num_threads(s->threads) schedule(static)") \
+  for (long n = 0; n < s->g.size; ++n) { body; }
+
+#define SPO_FOR_INTERIOR(body)                                                        \
+  {                                                                                   \
+    const long K0 = (s->d.dim == 3) ? BD : 0, K1 = (s->d.dim == 3) ? BD + s->d.n[2] : 1; \
+    const long plane = (long)s->d.n[1] * (K1 - K0);                                   \
+    _Pragma("omp parallel for num_threads(s->threads) schedule(static)")             \
+    for (long jk = 0; jk < plane; ++jk) {                                             \
+      long k = K0 + jk / s->d.n[1], j = BD + jk % s->d.n[1];                          \
+      for (long i = BD; i < BD + s->d.n[0]; ++i) {                                    \
+        long n = i + j * s->g.s[1] + k * s->g.s[2];                                   \
+        body;                                                                         \
+      }                                                                               \
+    }                                                                                 \
+  }
+
+/* One SolverFT iteration: halo refresh, all equations into dframe, then the
+ * forward-Euler step of every field. */
+static void spo_sys_step(spo_sys* s) {
+  const double* c = s->d.c;
+  const spo_stencil* st = &s->st;
+  for (int f = 0; f < s->nf; ++f) spo_update_halo(&s->d, &s->g, s->psi[f]);
+  double* p = s->psi[0];
+  double* q = s->psi[1];
+  double* t0 = s->tmp[0];
+  double* t1 = s->tmp[1];
+  double* d0 = s->dframe[0];
+  double* d1 = s->dframe[1];
+  switch (s->d.model) {
+    case SPO_MODEL_A:
+      /* printed scheme: V^2(psi) - psi^3 + psi  (c1 = c2 = 1) */
+      SPO_FOR_INTERIOR(d0[n] = spo_lap(st, p + n) + (-(c[1] * pow3(p[n])) + c[0] * p[n]));
+      break;
+    case SPO_MODEL_B:
+      /* printed scheme: -V^4(psi) + V^2(psi^3) - V^2(psi)  (c1 = c2 = 1) */
+      SPO_FOR_STORAGE(t0[n] = pow3(p[n]));
+      SPO_FOR_INTERIOR(d0[n] = -spo_bilap(st, p + n) +
+                               (c[1] * spo_lap(st, t0 + n) + -(c[0] * spo_lap(st, p + n))));
+      break;
+    case SPO_MODEL_C: {
+      /* psi: -V^4(psi) + V^2(psi^3) - V^2(psi) + V^2(g psi eta^2), g = 2 gamma = 2 c1
+       * eta: V^2(eta) + eta - eta^3 - g psi^2 eta                                   */
+      const double g = 2.0 * c[0];
+      SPO_FOR_STORAGE(t0[n] = pow3(p[n]); t1[n] = g * (p[n] * (q[n] * q[n])));
+      SPO_FOR_INTERIOR(
+          d0[n] = -spo_bilap(st, p + n) +
+                  (spo_lap(st, t0 + n) + (-spo_lap(st, p + n) + spo_lap(st, t1 + n)));
+          d1[n] = spo_lap(st, q + n) + (q[n] + (-pow3(q[n]) + -(g * ((p[n] * p[n]) * q[n])))));
+      break;
+    }
+    case SPO_MODEL_AMK:
+      /* M (kappa V^2(psi) - psi^3 + psi), M = c1, kappa = c2 */
+      SPO_FOR_INTERIOR(d0[n] = c[0] * (c[1] * spo_lap(st, p + n) + (-pow3(p[n]) + p[n])));
+      break;
+    case SPO_MODEL_BMK:
+      /* M (-kappa V^4(psi) + V^2(psi^3) - V^2(psi)) */
+      SPO_FOR_STORAGE(t0[n] = pow3(p[n]));
+      SPO_FOR_INTERIOR(d0[n] = c[0] * (-(c[1] * spo_bilap(st, p + n)) +
+                                       (spo_lap(st, t0 + n) + -spo_lap(st, p + n))));
+      break;
+    case SPO_OP_LAP: SPO_FOR_INTERIOR(d0[n] = spo_lap(st, p + n)); break;
+    case SPO_OP_BILAP: SPO_FOR_INTERIOR(d0[n] = spo_bilap(st, p + n)); break;
+    case SPO_OP_GRADLAP: SPO_FOR_INTERIOR(d0[n] = spo_gradlap_x(st, p + n)); break;
+    case SPO_OP_LAPCUBE:
+      SPO_FOR_STORAGE(t0[n] = pow3(p[n]));
+      SPO_FOR_INTERIOR(d0[n] = spo_lap(st, t0 + n));
+      break;
+    default: abort();
+  }
+  const double dt = s->d.dt;
+  for (int f = 0; f < s->nf; ++f) {
+    double* pf = s->psi[f];
+    double* df = s->dframe[f];
+    SPO_FOR_INTERIOR(pf[n] = pf[n] + dt * df[n]);
+  }
+}
+
+static void spo_copy_in(spo_sys* s, int f, const double* interior) {
+  const spo_geom* g = &s->g;
+  const long nz = (s->d.dim == 3) ? s->d.n[2] : 1;
+  for (long k = 0; k < nz; ++k)
+    for (long j = 0; j < s->d.n[1]; ++j)
+      memcpy(s->psi[f] + BD + (j + BD) * g->s[1] + (k + (s->d.dim == 3 ? BD : 0)) * g->s[2],
+             interior + (k * s->d.n[1] + j) * s->d.n[0], sizeof(double) * s->d.n[0]);
+}
+
+static void spo_copy_out(const spo_sys* s, double* const* src, int f, double* interior) {
+  const spo_geom* g = &s->g;
+  const long nz = (s->d.dim == 3) ? s->d.n[2] : 1;
+  for (long k = 0; k < nz; ++k)
+    for (long j = 0; j < s->d.n[1]; ++j)
+      memcpy(interior + (k * s->d.n[1] + j) * s->d.n[0],
+             src[f] + BD + (j + BD) * g->s[1] + (k + (s->d.dim == 3 ? BD : 0)) * g->s[2],
+             sizeof(double) * s->d.n[0]);
+}
+
+/* ------------------------------------------------------------------ */
+/* exported entry points                                               */
+/* ------------------------------------------------------------------ */
+
+int spo_fields(int model) { return spo_field_count(model); }
+
+/* Advance `fields` (nf interior arrays laid out back to back, x-fastest) by
+ * `nsteps` SolverFT iterations using `threads` OpenMP threads.  Returns 0. */
+int spo_run(const spo_desc* d, double* fields, int nsteps, int threads) {
+  spo_sys s;
+  spo_sys_init(&s, d, threads);
+  long cnt = (long)d->n[0] * d->n[1] * (d->dim == 3 ? d->n[2] : 1);
+  for (int f = 0; f < s.nf; ++f) spo_copy_in(&s, f, fields + f * cnt);
+  for (int it = 0; it < nsteps; ++it) spo_sys_step(&s);
+  for (int f = 0; f < s.nf; ++f) spo_copy_out(&s, s.psi, f, fields + f * cnt);
+  spo_sys_free(&s);
+  return 0;
+}
+
+/* Evaluate the right-hand side once (no step): dframe of every field. */
+int spo_rhs(const spo_desc* d, const double* fields, double* rhs) {
+  spo_sys s;
+  spo_sys_init(&s, d, 1);
+  long cnt = (long)d->n[0] * d->n[1] * (d->dim == 3 ? d->n[2] : 1);
+  for (int f = 0; f < s.nf; ++f) spo_copy_in(&s, f, fields + f * cnt);
+  spo_desc dd = *d;
+  dd.dt = 0.0; /* psi + 0*dframe leaves psi unchanged; dframe is what we want */
+  s.d = dd;
+  spo_sys_step(&s);
+  for (int f = 0; f < s.nf; ++f) spo_copy_out(&s, s.dframe, f, rhs + f * cnt);
+  spo_sys_free(&s);
+  return 0;
+}
+
+/* Run many independent systems (e.g. an ensemble) in parallel, one system per
+ * thread; descs[i] and field pointers ptrs[i] describe system i. */
+int spo_run_batch(const spo_desc* descs, double** ptrs, int count, const int* nsteps,
+                  int threads) {
+#pragma omp parallel for num_threads(threads > 0 ? threads : 1) schedule(dynamic, 1)
+  for (int i = 0; i < count; ++i) spo_run(&descs[i], ptrs[i], nsteps[i], 1);
+  return 0;
+}
+
+/* Sum of the interior values (Kahan-free plain double sum, x-fastest order). */
+double spo_mass(const double* interior, long long count) {
+  double m = 0.0;
+  for (long long i = 0; i < count; ++i) m += interior[i];
+  return m;
+}
+
+int spo_omp_max_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}

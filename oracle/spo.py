@@ -1,0 +1,122 @@
+"""ctypes wrapper of the CPU oracle (oracle/spo.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, and only as the checker.  The product path never
+imports this module.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+MODEL_A, MODEL_B, MODEL_C, MODEL_AMK, MODEL_BMK = 0, 1, 2, 3, 4
+OP_LAP, OP_BILAP, OP_GRADLAP, OP_LAPCUBE = 10, 11, 12, 13
+PERIODIC, DIRICHLET = 0, 1
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int),
+        ("n", ctypes.c_int * 3),
+        ("model", ctypes.c_int),
+        ("lap_pts", ctypes.c_int),
+        ("gradlap_pts", ctypes.c_int),
+        ("bilap_pts", ctypes.c_int),
+        ("h", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("c", ctypes.c_double * 8),
+        ("bc", ctypes.c_int * 6),
+        ("bcv", ctypes.c_double * 6),
+    ]
+
+
+def _load():
+    path = os.path.join(_HERE, "libspo.so")
+    if not os.path.exists(path):
+        raise ImportError("oracle library %s is missing; run `make -C oracle`" % path)
+    lib = ctypes.CDLL(path)
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.spo_run.argtypes = [ctypes.POINTER(Desc), dp, ctypes.c_int, ctypes.c_int]
+    lib.spo_rhs.argtypes = [ctypes.POINTER(Desc), dp, dp]
+    lib.spo_seed_uniform.argtypes = [ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_longlong, ctypes.c_longlong, dp]
+    lib.spo_fields.argtypes = [ctypes.c_int]
+    lib.spo_mass.argtypes = [dp, ctypes.c_longlong]
+    lib.spo_mass.restype = ctypes.c_double
+    lib.spo_run_batch.argtypes = [ctypes.POINTER(Desc), ctypes.POINTER(dp), ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+    lib.spo_omp_max_threads.restype = ctypes.c_int
+    return lib
+
+
+_lib = _load()
+
+
+def make_desc(dim, n, model, h, dt, coeff=(), stencil=None, bc=PERIODIC, bcv=0.0):
+    d = Desc()
+    d.dim = dim
+    nn = list(n) + [1] * (3 - len(n))
+    for i in range(3):
+        d.n[i] = nn[i]
+    d.model = model
+    if stencil is None:
+        stencil = (5, 6, 13) if dim == 2 else (7, 10, 25)
+    d.lap_pts, d.gradlap_pts, d.bilap_pts = stencil
+    d.h = h
+    d.dt = dt
+    cs = list(coeff) + [1.0] * (8 - len(coeff))
+    for i in range(8):
+        d.c[i] = cs[i]
+    bcs = bc if isinstance(bc, (list, tuple)) else [bc] * 6
+    vals = bcv if isinstance(bcv, (list, tuple)) else [bcv] * 6
+    for i in range(6):
+        d.bc[i] = bcs[i]
+        d.bcv[i] = vals[i]
+    return d
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def nfields(model):
+    return _lib.spo_fields(model)
+
+
+def shape_of(d):
+    return (d.n[2], d.n[1], d.n[0]) if d.dim == 3 else (d.n[1], d.n[0])
+
+
+def run(d, fields, steps, threads=1):
+    """Advance `fields` (array (nf, *shape) or (*shape), float64) by `steps`."""
+    a = np.ascontiguousarray(fields, dtype=np.float64).copy()
+    _lib.spo_run(ctypes.byref(d), _ptr(a), int(steps), int(threads))
+    return a
+
+
+def rhs(d, fields):
+    a = np.ascontiguousarray(fields, dtype=np.float64)
+    out = np.empty_like(a)
+    _lib.spo_rhs(ctypes.byref(d), _ptr(a), _ptr(out))
+    return out
+
+
+def seed_uniform(seed, lo, hi, count, first=0):
+    out = np.empty(int(count), dtype=np.float64)
+    _lib.spo_seed_uniform(ctypes.c_uint64(seed), lo, hi, int(count), int(first), _ptr(out))
+    return out
+
+
+def run_batch(descs, fields_list, steps_list, threads):
+    """Run independent systems in parallel (one per thread).  Modifies arrays in place."""
+    k = len(descs)
+    arr = (Desc * k)(*descs)
+    ptrs = (ctypes.POINTER(ctypes.c_double) * k)(*[_ptr(f) for f in fields_list])
+    steps = (ctypes.c_int * k)(*[int(s) for s in steps_list])
+    _lib.spo_run_batch(arr, ptrs, k, steps, int(threads))
+
+
+def max_threads():
+    return _lib.spo_omp_max_threads()

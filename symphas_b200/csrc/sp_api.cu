@@ -1,0 +1,763 @@
+/*
+ * sp_api.cu -- implementation of the C ABI declared in include/symphas_b200.h.
+ *
+ * Host-side plumbing only: validation, device buffers, TMA descriptors, the
+ * step loop (with CUDA-graph replay of long step sequences), uploads,
+ * downloads and reductions.  The numerical work is in the kernels of
+ * sp_kernels.cuh, instantiated in sp_inst_*.cu.
+ */
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/symphas_b200.h"
+#include "sp_kernels.cuh"
+#include "sp_registry.h"
+
+namespace sp {
+
+// ---------------------------------------------------------------------------
+// kernel registry
+// ---------------------------------------------------------------------------
+namespace {
+using KeyT = std::tuple<int, int, int, int, int, int, int>;
+std::map<KeyT, KernelInfo>& table() {
+  static std::map<KeyT, KernelInfo> t;
+  return t;
+}
+KeyT tup(const KernelKey& k) { return KeyT{k.model, k.form, k.dim, k.dtype, k.lp, k.gp, k.bp}; }
+}  // namespace
+
+void register_kernel(const KernelKey& key, const KernelInfo& info) { table()[tup(key)] = info; }
+const KernelInfo* find_kernel(const KernelKey& key) {
+  auto it = table().find(tup(key));
+  return it == table().end() ? nullptr : &it->second;
+}
+void register_exact_kernels();
+void register_fused_kernels();
+void register_all_kernels() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    register_exact_kernels();
+    register_fused_kernels();
+  });
+}
+
+// ---------------------------------------------------------------------------
+// seeded initial values: SplitMix64 counter stream, bit-identical to the oracle
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_seed(T* org, int dim, int n0, int n1, int n2, int h0, int h1, int h2,
+                       long long pitch, long long plane, unsigned long long seed, double lo,
+                       double hi) {
+  const long long total = (long long)n0 * n1 * (dim == 3 ? n2 : 1);
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+       id += (long long)gridDim.x * blockDim.x) {
+    unsigned long long z = seed + (unsigned long long)(id + 1) * 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    const double u = __dmul_rn(double(z >> 11), 1.0 / 9007199254740992.0);
+    const double v = __dadd_rn(lo, __dmul_rn(__dsub_rn(hi, lo), u));
+    const long long i = id % n0, j = (id / n0) % n1, k = id / ((long long)n0 * n1);
+    org[(k + (dim == 3 ? h2 : 0)) * plane + (j + h1) * pitch + (i + h0)] = T(v);
+  }
+}
+
+}  // namespace sp
+
+// ---------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------
+struct sp_handle {
+  sp_desc d{};
+  const sp::KernelInfo* ki = nullptr;
+  int nf = 1, batch = 1, dim = 2;
+  int n[3] = {1, 1, 1}, h[3] = {0, 0, 0};
+  long long pitch = 0, ly = 0, lz = 1, plane = 0, felems = 0;
+  size_t esz = 8;
+  char* buf[2] = {nullptr, nullptr};
+  CUtensorMap* maps_d[2] = {nullptr, nullptr};
+  void** outs_d[2] = {nullptr, nullptr};
+  int cur = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sms = 148;
+  // 3D grid
+  int ntx = 1, nty = 1, nzc = 1, zchunk = 1;
+  // 2D persistent grid
+  void* inst2_d = nullptr;
+  int2* items_d = nullptr;
+  int nitems = 0;
+  int* ctr_d = nullptr;
+  int grid2 = 1;
+  // scratch for reductions
+  double* partial_d = nullptr;
+  size_t partial_n = 0;
+  double* result_d = nullptr;
+  double* result_h = nullptr;
+  int* err_d = nullptr;
+  // graphs replaying GRAPH_STEPS steps from each buffer parity
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  bool graphs = true;  // false once capture failed on this stream
+  long long launches = 0;
+  std::string err;
+};
+
+namespace {
+
+constexpr int GRAPH_STEPS = 32;
+constexpr int RED_THREADS = 256;
+
+thread_local std::string g_create_error;
+
+int fail(sp_handle* H, int code, const std::string& msg) {
+  if (H) H->err = msg;
+  return code;
+}
+int cuda_fail(sp_handle* H, cudaError_t e, const char* what) {
+  return fail(H, SP_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define SP_CUDA(H, call)                              \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) return cuda_fail(H, e_, #call); \
+  } while (0)
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiled) nullptr;
+    return reinterpret_cast<EncodeTiled>(p);
+  }();
+  return fn;
+}
+
+int energy_kind(int model) {
+  switch (model) {
+    case SP_MODEL_AMK:
+    case SP_MODEL_BMK: return 1;
+    case SP_MODEL_C: return 2;
+    default: return 0;
+  }
+}
+
+char* field_base(sp_handle* H, int which, int inst, int f) {
+  return H->buf[which] + size_t(inst * H->nf + f) * H->felems * H->esz;
+}
+char* field_origin(sp_handle* H, int which, int inst, int f) {
+  return field_base(H, which, inst, f) +
+         size_t((H->dim == 3 ? H->h[2] : 0) * H->plane + H->h[1] * H->pitch + H->h[0]) * H->esz;
+}
+
+int check_err_flag(sp_handle* H) {
+  int e = 0;
+  SP_CUDA(H, cudaMemcpyAsync(&e, H->err_d, sizeof(int), cudaMemcpyDeviceToHost, H->stream));
+  SP_CUDA(H, cudaStreamSynchronize(H->stream));
+  if (e != 0) {
+    cudaMemsetAsync(H->err_d, 0, sizeof(int), H->stream);
+    return fail(H, SP_ETIMEOUT, "a kernel gave up waiting for a TMA tile (device error flag set)");
+  }
+  return SP_OK;
+}
+
+template <class T>
+int launch_step_t(sp_handle* H, int rhs_only, double* partial) {
+  const int src = H->cur, dst = H->cur ^ 1;
+  const double divh = 1.0 / H->d.h;
+  const double divh2 = divh * divh, divh3 = divh * divh2, divh4 = divh2 * divh2;
+  cudaError_t e;
+  if (H->dim == 3) {
+    sp::StepParams<T> p{};
+    p.maps = H->maps_d[src];
+    p.out = reinterpret_cast<T* const*>(H->outs_d[dst]);
+    for (int a = 0; a < 3; ++a) {
+      p.n[a] = H->n[a];
+      p.h[a] = H->h[a];
+      p.per[a] = H->d.boundary[2 * a] == SP_PERIODIC;
+    }
+    p.pitch = H->pitch;
+    p.plane = H->plane;
+    p.ntx = H->ntx;
+    p.nty = H->nty;
+    p.zchunk = H->zchunk;
+    p.rhs_only = rhs_only;
+    p.dt = T(H->d.dt);
+    p.divh2 = T(divh2);
+    p.divh3 = T(divh3);
+    p.divh4 = T(divh4);
+    for (int i = 0; i < 8; ++i) p.coef[i] = T(H->d.coeff[i]);
+    p.partial = partial;
+    p.err = H->err_d;
+    e = H->ki->launch(&p, dim3(H->ntx * H->nty, H->nzc, H->batch), H->stream);
+  } else {
+    sp::Step2Params<T> p{};
+    p.maps = H->maps_d[src];
+    p.out = reinterpret_cast<T* const*>(H->outs_d[dst]);
+    p.inst = static_cast<const sp::Inst2<T>*>(H->inst2_d);
+    p.items = H->items_d;
+    p.nitems = H->nitems;
+    p.ctr = H->ctr_d;
+    p.rhs_only = rhs_only;
+    p.hx = H->h[0];
+    p.hy = H->h[1];
+    p.partial = partial;
+    p.err = H->err_d;
+    e = H->ki->launch(&p, dim3(H->grid2), H->stream);
+  }
+  if (e != cudaSuccess) return cuda_fail(H, e, "fused step launch");
+  ++H->launches;
+  if (!rhs_only) H->cur = dst;
+  return SP_OK;
+}
+
+int launch_step(sp_handle* H, int rhs_only, double* partial) {
+  return H->esz == 4 ? launch_step_t<float>(H, rhs_only, partial)
+                     : launch_step_t<double>(H, rhs_only, partial);
+}
+
+template <class T>
+int fill_halo_t(sp_handle* H, int which, int inst, int f) {
+  sp::HaloParams<T> p{};
+  p.org = reinterpret_cast<T*>(field_base(H, which, inst, f));
+  p.dim = H->dim;
+  for (int a = 0; a < 3; ++a) {
+    p.n[a] = H->n[a];
+    p.h[a] = H->h[a];
+  }
+  p.pitch = H->pitch;
+  p.plane = H->plane;
+  for (int s = 0; s < 6; ++s) {
+    p.bc[s] = H->d.boundary[s];
+    p.bv[s] = T(H->d.boundary_value[s]);
+  }
+  sp::k_fill_halo<T><<<H->sms * 4, 256, 0, H->stream>>>(p);
+  SP_CUDA(H, cudaGetLastError());
+  return SP_OK;
+}
+
+int fill_halo(sp_handle* H, int which, int inst, int f) {
+  return H->esz == 4 ? fill_halo_t<float>(H, which, inst, f)
+                     : fill_halo_t<double>(H, which, inst, f);
+}
+
+// after new interior values: the halo of the current buffer, and the constant
+// (Dirichlet) halo of the other buffer, which the step kernels never write
+int refresh_halos(sp_handle* H, int inst, int f) {
+  if (int rc = fill_halo(H, H->cur ^ 1, inst, f)) return rc;
+  return fill_halo(H, H->cur, inst, f);
+}
+
+int validate(const sp_desc* d, std::string& why) {
+  if (!d) return why = "null description", SP_EINVAL;
+  if (d->dim != 2 && d->dim != 3) return why = "dim must be 2 or 3", SP_EINVAL;
+  for (int a = 0; a < d->dim; ++a)
+    if (d->n[a] < 4 || d->n[a] > (1 << 16)) return why = "each extent must be in [4, 65536]", SP_EINVAL;
+  if (d->dtype != SP_F32 && d->dtype != SP_F64) return why = "dtype must be SP_F32 or SP_F64", SP_EINVAL;
+  if (d->form != SP_FORM_EXACT && d->form != SP_FORM_FUSED) return why = "form must be exact or fused", SP_EINVAL;
+  if (!(d->h > 0.0)) return why = "grid spacing h must be positive", SP_EINVAL;
+  if (d->batch < 1) return why = "batch must be >= 1", SP_EINVAL;
+  for (int a = 0; a < d->dim; ++a) {
+    const int l = d->boundary[2 * a], r = d->boundary[2 * a + 1];
+    if ((l != SP_PERIODIC && l != SP_DIRICHLET) || (r != SP_PERIODIC && r != SP_DIRICHLET))
+      return why = "boundary must be SP_PERIODIC or SP_DIRICHLET", SP_EINVAL;
+    if ((l == SP_PERIODIC) != (r == SP_PERIODIC))
+      return why = "a periodic axis must be periodic on both sides", SP_EINVAL;
+  }
+  return SP_OK;
+}
+
+void release(sp_handle* H) {
+  if (!H) return;
+  if (H->stream) cudaStreamSynchronize(H->stream);
+  for (int k = 0; k < 2; ++k) {
+    if (H->gexec[k]) cudaGraphExecDestroy(H->gexec[k]);
+    cudaFree(H->buf[k]);
+    cudaFree(H->maps_d[k]);
+    cudaFree(H->outs_d[k]);
+  }
+  cudaFree(H->inst2_d);
+  cudaFree(H->items_d);
+  cudaFree(H->ctr_d);
+  cudaFree(H->partial_d);
+  cudaFree(H->result_d);
+  cudaFree(H->err_d);
+  if (H->result_h) cudaFreeHost(H->result_h);
+  if (H->own_stream && H->stream) cudaStreamDestroy(H->stream);
+  delete H;
+}
+
+template <class T>
+int setup_2d_t(sp_handle* H) {
+  std::vector<sp::Inst2<T>> ip(H->batch);
+  const double divh = 1.0 / H->d.h;
+  const double divh2 = divh * divh, divh3 = divh * divh2, divh4 = divh2 * divh2;
+  for (int i = 0; i < H->batch; ++i) {
+    sp::Inst2<T>& q = ip[i];
+    q.n[0] = H->n[0];
+    q.n[1] = H->n[1];
+    q.per[0] = H->d.boundary[0] == SP_PERIODIC;
+    q.per[1] = H->d.boundary[2] == SP_PERIODIC;
+    q.pitch = H->pitch;
+    q.ntx = H->ntx;
+    q.kind = 0;
+    q.dt = T(H->d.dt);
+    q.divh2 = T(divh2);
+    q.divh3 = T(divh3);
+    q.divh4 = T(divh4);
+    for (int c = 0; c < 8; ++c) q.coef[c] = T(H->d.coeff[c]);
+  }
+  SP_CUDA(H, cudaMalloc(&H->inst2_d, sizeof(sp::Inst2<T>) * H->batch));
+  SP_CUDA(H, cudaMemcpy(H->inst2_d, ip.data(), sizeof(sp::Inst2<T>) * H->batch,
+                        cudaMemcpyHostToDevice));
+  const int tiles = H->ntx * H->nty;
+  H->nitems = tiles * H->batch;
+  if (H->batch > 1) {
+    std::vector<int2> items(H->nitems);
+    for (int i = 0; i < H->batch; ++i)
+      for (int t = 0; t < tiles; ++t) items[size_t(i) * tiles + t] = make_int2(i, t);
+    SP_CUDA(H, cudaMalloc(&H->items_d, sizeof(int2) * items.size()));
+    SP_CUDA(H, cudaMemcpy(H->items_d, items.data(), sizeof(int2) * items.size(),
+                          cudaMemcpyHostToDevice));
+  }
+  SP_CUDA(H, cudaMalloc(&H->ctr_d, 2 * sizeof(int)));
+  SP_CUDA(H, cudaMemset(H->ctr_d, 0, 2 * sizeof(int)));
+  const int occ = H->ki->occupancy();
+  H->grid2 = std::max(1, std::min(H->sms * occ, H->nitems));
+  return SP_OK;
+}
+
+int create(const sp_desc* desc, sp_handle* H) {
+  std::string why;
+  if (int rc = validate(desc, why)) return fail(H, rc, why);
+  sp::register_all_kernels();
+  H->d = *desc;
+  H->dim = desc->dim;
+  H->batch = desc->batch;
+  H->esz = desc->dtype == SP_F32 ? 4 : 8;
+  const sp::KernelKey key{desc->model, desc->form, desc->dim, desc->dtype,
+                          desc->lap_pts, desc->gradlap_pts, desc->bilap_pts};
+  H->ki = sp::find_kernel(key);
+  if (!H->ki) {
+    char b[256];
+    snprintf(b, sizeof b,
+             "no fused kernel built for model %d form %d dim %d dtype %d stencil <%d,%d,%d>",
+             desc->model, desc->form, desc->dim, desc->dtype, desc->lap_pts,
+             desc->gradlap_pts, desc->bilap_pts);
+    return fail(H, SP_EINVAL, b);
+  }
+  H->nf = H->ki->nf;
+  for (int a = 0; a < 3; ++a) H->n[a] = (a < H->dim) ? desc->n[a] : 1;
+  const int R = H->ki->R;
+  for (int a = 0; a < H->dim; ++a)
+    if (H->n[a] < 2 * R) return fail(H, SP_EINVAL, "an extent is smaller than twice the stencil reach");
+  H->h[0] = H->ki->hx;
+  H->h[1] = R;
+  H->h[2] = H->dim == 3 ? R : 0;
+  const int va = int(16 / H->esz);
+  H->pitch = ((H->n[0] + 2 * H->h[0] + va - 1) / va) * va;
+  H->ly = H->n[1] + 2 * H->h[1];
+  H->lz = H->dim == 3 ? H->n[2] + 2 * H->h[2] : 1;
+  H->plane = H->pitch * H->ly;
+  H->felems = ((H->plane * H->lz + 63) / 64) * 64;
+  H->ntx = (H->n[0] + H->ki->tx - 1) / H->ki->tx;
+  H->nty = (H->n[1] + H->ki->ty - 1) / H->ki->ty;
+
+  int dev = 0;
+  SP_CUDA(H, cudaGetDevice(&dev));
+  SP_CUDA(H, cudaDeviceGetAttribute(&H->sms, cudaDevAttrMultiProcessorCount, dev));
+  SP_CUDA(H, cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking));
+  H->own_stream = true;
+
+  const size_t bytes = size_t(H->batch) * H->nf * H->felems * H->esz;
+  for (int k = 0; k < 2; ++k) {
+    if (cudaMalloc(&H->buf[k], bytes) != cudaSuccess)
+      return fail(H, SP_ENOMEM, "device allocation of the field buffers failed");
+    SP_CUDA(H, cudaMemset(H->buf[k], 0, bytes));
+  }
+
+  // TMA descriptors of every field of both buffers, and output origins
+  EncodeTiled enc = encode_fn();
+  if (!enc) return fail(H, SP_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  const int cnt = H->batch * H->nf;
+  for (int k = 0; k < 2; ++k) {
+    std::vector<CUtensorMap> maps(cnt);
+    std::vector<void*> outs(cnt);
+    for (int i = 0; i < H->batch; ++i)
+      for (int f = 0; f < H->nf; ++f) {
+        const int idx = i * H->nf + f;
+        void* base = field_base(H, k, i, f);
+        outs[idx] = base;
+        const cuuint32_t bw = cuuint32_t(H->ki->tx + 2 * H->h[0]);
+        const cuuint32_t bh = cuuint32_t(H->ki->ty + 2 * R);
+        const CUtensorMapDataType dt =
+            H->esz == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+        CUresult r;
+        if (H->dim == 3) {
+          cuuint64_t gdim[3] = {cuuint64_t(H->pitch), cuuint64_t(H->ly), cuuint64_t(H->lz)};
+          cuuint64_t gstr[2] = {cuuint64_t(H->pitch * H->esz), cuuint64_t(H->plane * H->esz)};
+          cuuint32_t box[3] = {bw, bh, 1};
+          cuuint32_t es[3] = {1, 1, 1};
+          r = enc(&maps[idx], dt, 3, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        } else {
+          cuuint64_t gdim[2] = {cuuint64_t(H->pitch), cuuint64_t(H->ly)};
+          cuuint64_t gstr[1] = {cuuint64_t(H->pitch * H->esz)};
+          cuuint32_t box[2] = {bw, bh};
+          cuuint32_t es[2] = {1, 1};
+          r = enc(&maps[idx], dt, 2, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        }
+        if (r != CUDA_SUCCESS) {
+          char b[128];
+          snprintf(b, sizeof b, "cuTensorMapEncodeTiled failed (CUresult %d)", int(r));
+          return fail(H, SP_ECUDA, b);
+        }
+      }
+    SP_CUDA(H, cudaMalloc(&H->maps_d[k], sizeof(CUtensorMap) * cnt));
+    SP_CUDA(H, cudaMemcpy(H->maps_d[k], maps.data(), sizeof(CUtensorMap) * cnt,
+                          cudaMemcpyHostToDevice));
+    SP_CUDA(H, cudaMalloc(&H->outs_d[k], sizeof(void*) * cnt));
+    SP_CUDA(H, cudaMemcpy(H->outs_d[k], outs.data(), sizeof(void*) * cnt, cudaMemcpyHostToDevice));
+  }
+
+  size_t partial_n = 2 * size_t(H->sms) * 8;
+  if (H->dim == 3) {
+    // z planes per CTA: aim for at least ~4 waves of resident CTAs, but keep
+    // chunks long enough that the 2R prologue planes stay a small overhead
+    const int occ = H->ki->occupancy();
+    const long long tiles = (long long)H->ntx * H->nty * H->batch;
+    const long long want = 4LL * H->sms * occ;
+    int chunks = int((want + tiles - 1) / tiles);
+    chunks = std::max(1, std::min(chunks, std::max(1, H->n[2] / std::max(8, 4 * R))));
+    H->zchunk = (H->n[2] + chunks - 1) / chunks;
+    if (const char* zc = getenv("SP_ZCHUNK")) {
+      const int v = atoi(zc);
+      if (v > 0) H->zchunk = std::min(v, H->n[2]);
+    }
+    H->nzc = (H->n[2] + H->zchunk - 1) / H->zchunk;
+    partial_n = std::max(partial_n, size_t(H->ntx) * H->nty * H->nzc * H->batch);
+  } else {
+    int rc = H->esz == 4 ? setup_2d_t<float>(H) : setup_2d_t<double>(H);
+    if (rc) return rc;
+    partial_n = std::max(partial_n, size_t(H->grid2));
+  }
+  H->partial_n = partial_n;
+  SP_CUDA(H, cudaMalloc(&H->partial_d, sizeof(double) * partial_n));
+  SP_CUDA(H, cudaMalloc(&H->result_d, sizeof(double) * (2 + H->batch)));
+  SP_CUDA(H, cudaMallocHost(&H->result_h, sizeof(double) * (2 + H->batch)));
+  SP_CUDA(H, cudaMalloc(&H->err_d, sizeof(int)));
+  SP_CUDA(H, cudaMemset(H->err_d, 0, sizeof(int)));
+  SP_CUDA(H, cudaDeviceSynchronize());
+  return SP_OK;
+}
+
+int check_field(sp_handle* H, int inst, int field, size_t bytes) {
+  if (!H) return SP_EINVAL;
+  if (inst < 0 || inst >= H->batch) return fail(H, SP_EINVAL, "instance index out of range");
+  if (field < 0 || field >= H->nf) return fail(H, SP_EINVAL, "field index out of range");
+  const size_t need = size_t(H->n[0]) * H->n[1] * (H->dim == 3 ? H->n[2] : 1) * H->esz;
+  if (bytes != need) return fail(H, SP_EINVAL, "byte count does not match the interior size");
+  return SP_OK;
+}
+
+cudaMemcpy3DParms interior_copy(sp_handle* H, int which, int inst, int field, void* other,
+                                bool to_device, cudaMemcpyKind kind) {
+  cudaMemcpy3DParms p{};
+  cudaPitchedPtr dev = make_cudaPitchedPtr(field_base(H, which, inst, field), H->pitch * H->esz,
+                                           H->pitch, H->ly);
+  cudaPitchedPtr com = make_cudaPitchedPtr(other, H->n[0] * H->esz, H->n[0], H->n[1]);
+  cudaPos dpos = make_cudaPos(H->h[0] * H->esz, H->h[1], H->dim == 3 ? H->h[2] : 0);
+  if (to_device) {
+    p.srcPtr = com;
+    p.dstPtr = dev;
+    p.dstPos = dpos;
+  } else {
+    p.srcPtr = dev;
+    p.srcPos = dpos;
+    p.dstPtr = com;
+  }
+  p.extent = make_cudaExtent(H->n[0] * H->esz, H->n[1], H->dim == 3 ? H->n[2] : 1);
+  p.kind = kind;
+  return p;
+}
+
+int upload(sp_handle* H, int inst, int field, const void* src, size_t bytes, cudaMemcpyKind k) {
+  if (int rc = check_field(H, inst, field, bytes)) return rc;
+  cudaMemcpy3DParms p = interior_copy(H, H->cur, inst, field, const_cast<void*>(src), true, k);
+  SP_CUDA(H, cudaMemcpy3DAsync(&p, H->stream));
+  return refresh_halos(H, inst, field);
+}
+
+int download(sp_handle* H, int which, int inst, int field, void* dst, size_t bytes,
+             cudaMemcpyKind k, bool wait) {
+  if (int rc = check_field(H, inst, field, bytes)) return rc;
+  cudaMemcpy3DParms p = interior_copy(H, which, inst, field, dst, false, k);
+  SP_CUDA(H, cudaMemcpy3DAsync(&p, H->stream));
+  if (wait) return check_err_flag(H);
+  return SP_OK;
+}
+
+int capture_graph(sp_handle* H) {
+  const int parity = H->cur;
+  cudaGraph_t g = nullptr;
+  if (H->stream == nullptr || cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeThreadLocal) !=
+                                  cudaSuccess) {
+    cudaGetLastError();
+    H->graphs = false;  // e.g. the legacy default stream cannot be captured
+    return SP_OK;
+  }
+  int rc = SP_OK;
+  const long long before = H->launches;
+  for (int i = 0; i < GRAPH_STEPS && rc == SP_OK; ++i) rc = launch_step(H, 0, nullptr);
+  cudaError_t e = cudaStreamEndCapture(H->stream, &g);
+  H->launches = before;
+  H->cur = parity;
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(H, e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&H->gexec[parity], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(H, e, "cudaGraphInstantiate");
+  return SP_OK;
+}
+
+template <class T>
+int reduce_t(sp_handle* H, int inst, int field, double* mass, double* energy) {
+  sp::ReduceParams<T> p{};
+  p.f0 = reinterpret_cast<const T*>(field_base(H, H->cur, inst, field));
+  p.e0 = reinterpret_cast<const T*>(field_base(H, H->cur, inst, 0));
+  p.e1 = H->nf > 1 ? reinterpret_cast<const T*>(field_base(H, H->cur, inst, 1)) : nullptr;
+  p.dim = H->dim;
+  for (int a = 0; a < 3; ++a) {
+    p.n[a] = H->n[a];
+    p.h[a] = H->h[a];
+  }
+  p.pitch = H->pitch;
+  p.plane = H->plane;
+  p.energy_kind = energy_kind(H->d.model);
+  p.c1 = H->d.coeff[0];
+  p.c2 = H->d.coeff[1];
+  p.kappa = H->d.model == SP_MODEL_C ? 1.0 : H->d.coeff[1];
+  p.gamma = H->d.coeff[0];
+  p.h_sp = H->d.h;
+  p.partial = H->partial_d;
+  const long long total = (long long)H->n[0] * H->n[1] * (H->dim == 3 ? H->n[2] : 1);
+  int blocks = int(std::min<long long>((total + RED_THREADS - 1) / RED_THREADS,
+                                       (long long)(H->partial_n / 2)));
+  blocks = std::max(blocks, 1);
+  sp::k_reduce<T, RED_THREADS><<<blocks, RED_THREADS, 0, H->stream>>>(p);
+  SP_CUDA(H, cudaGetLastError());
+  sp::k_finish<RED_THREADS><<<1, RED_THREADS, 0, H->stream>>>(H->partial_d, blocks, 2, H->result_d);
+  SP_CUDA(H, cudaGetLastError());
+  SP_CUDA(H, cudaMemcpyAsync(H->result_h, H->result_d, 2 * sizeof(double),
+                             cudaMemcpyDeviceToHost, H->stream));
+  if (int rc = check_err_flag(H)) return rc;
+  double hd = 1.0;
+  for (int a = 0; a < H->dim; ++a) hd *= H->d.h;
+  if (mass) *mass = H->result_h[0];
+  if (energy) *energy = H->result_h[1] * hd;
+  if (!std::isfinite(H->result_h[0]) || !std::isfinite(H->result_h[1]))
+    return fail(H, SP_ENONFINITE, "the field holds NaN or Inf");
+  return SP_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int sp_create(const sp_desc* desc, sp_handle** out) {
+  g_create_error.clear();
+  if (!out) return SP_EINVAL;
+  *out = nullptr;
+  sp_handle* H = new sp_handle();
+  int rc = create(desc, H);
+  if (rc != SP_OK) {
+    g_create_error = H->err;
+    release(H);
+    return rc;
+  }
+  *out = H;
+  return SP_OK;
+}
+
+const char* sp_create_error(void) { return g_create_error.c_str(); }
+
+int sp_upload(sp_handle* h, int inst, int field, const void* host, size_t bytes) {
+  if (!h || !host) return SP_EINVAL;
+  return upload(h, inst, field, host, bytes, cudaMemcpyHostToDevice);
+}
+
+int sp_upload_device(sp_handle* h, int inst, int field, const void* dev, size_t bytes) {
+  if (!h || !dev) return SP_EINVAL;
+  return upload(h, inst, field, dev, bytes, cudaMemcpyDeviceToDevice);
+}
+
+int sp_fill_uniform(sp_handle* H, int inst, int field, uint64_t seed, double lo, double hi) {
+  if (!H) return SP_EINVAL;
+  const size_t bytes = size_t(H->n[0]) * H->n[1] * (H->dim == 3 ? H->n[2] : 1) * H->esz;
+  if (int rc = check_field(H, inst, field, bytes)) return rc;
+  char* base = field_base(H, H->cur, inst, field);
+  if (H->esz == 4)
+    sp::k_seed<float><<<H->sms * 4, 256, 0, H->stream>>>(
+        reinterpret_cast<float*>(base), H->dim, H->n[0], H->n[1], H->n[2], H->h[0], H->h[1],
+        H->h[2], H->pitch, H->plane, seed, lo, hi);
+  else
+    sp::k_seed<double><<<H->sms * 4, 256, 0, H->stream>>>(
+        reinterpret_cast<double*>(base), H->dim, H->n[0], H->n[1], H->n[2], H->h[0], H->h[1],
+        H->h[2], H->pitch, H->plane, seed, lo, hi);
+  SP_CUDA(H, cudaGetLastError());
+  return refresh_halos(H, inst, field);
+}
+
+int sp_step(sp_handle* H, int nsteps) {
+  if (!H || nsteps < 0) return SP_EINVAL;
+  while (nsteps > 0) {
+    if (nsteps >= GRAPH_STEPS && H->graphs && !H->gexec[H->cur])
+      if (int rc = capture_graph(H)) return rc;
+    if (nsteps >= GRAPH_STEPS && H->gexec[H->cur]) {
+      SP_CUDA(H, cudaGraphLaunch(H->gexec[H->cur], H->stream));
+      H->launches += GRAPH_STEPS;
+      nsteps -= GRAPH_STEPS;
+    } else {
+      if (int rc = launch_step(H, 0, nullptr)) return rc;
+      --nsteps;
+    }
+  }
+  return SP_OK;
+}
+
+int sp_step_mass(sp_handle* H, int nsteps, double* mass) {
+  if (!H || nsteps < 1 || !mass) return SP_EINVAL;
+  if (H->dim == 2 && H->batch > 1)
+    return fail(H, SP_EINVAL, "fused mass reduction needs dim 3 or a single 2D instance");
+  if (int rc = sp_step(H, nsteps - 1)) return rc;
+  if (int rc = launch_step(H, 0, H->partial_d)) return rc;
+  const int per = H->dim == 3 ? H->ntx * H->nty * H->nzc : H->grid2;
+  for (int i = 0; i < H->batch; ++i) {
+    sp::k_finish<RED_THREADS><<<1, RED_THREADS, 0, H->stream>>>(H->partial_d + size_t(i) * per,
+                                                               per, 1, H->result_d + i);
+    SP_CUDA(H, cudaGetLastError());
+  }
+  SP_CUDA(H, cudaMemcpyAsync(H->result_h, H->result_d, sizeof(double) * H->batch,
+                             cudaMemcpyDeviceToHost, H->stream));
+  if (int rc = check_err_flag(H)) return rc;
+  for (int i = 0; i < H->batch; ++i) mass[i] = H->result_h[i];
+  return SP_OK;
+}
+
+int sp_eval_rhs(sp_handle* H, int inst, int field, void* host, size_t bytes) {
+  if (!H || !host) return SP_EINVAL;
+  if (int rc = check_field(H, inst, field, bytes)) return rc;
+  if (int rc = launch_step(H, 1, nullptr)) return rc;
+  return download(H, H->cur ^ 1, inst, field, host, bytes, cudaMemcpyDeviceToHost, true);
+}
+
+int sp_download(sp_handle* h, int inst, int field, void* host, size_t bytes) {
+  if (!h || !host) return SP_EINVAL;
+  return download(h, h->cur, inst, field, host, bytes, cudaMemcpyDeviceToHost, true);
+}
+
+int sp_download_device(sp_handle* h, int inst, int field, void* dev, size_t bytes) {
+  if (!h || !dev) return SP_EINVAL;
+  return download(h, h->cur, inst, field, dev, bytes, cudaMemcpyDeviceToDevice, false);
+}
+
+int sp_reduce(sp_handle* H, int inst, int field, double* mass, double* energy) {
+  if (!H) return SP_EINVAL;
+  if (inst < 0 || inst >= H->batch || field < 0 || field >= H->nf)
+    return fail(H, SP_EINVAL, "instance or field index out of range");
+  return H->esz == 4 ? reduce_t<float>(H, inst, field, mass, energy)
+                     : reduce_t<double>(H, inst, field, mass, energy);
+}
+
+int sp_set_dt(sp_handle* H, double dt) {
+  if (!H) return SP_EINVAL;
+  if (!std::isfinite(dt)) return fail(H, SP_EINVAL, "dt must be finite");
+  if (dt == H->d.dt) return SP_OK;
+  SP_CUDA(H, cudaStreamSynchronize(H->stream));
+  H->d.dt = dt;
+  for (int k = 0; k < 2; ++k)
+    if (H->gexec[k]) {
+      cudaGraphExecDestroy(H->gexec[k]);
+      H->gexec[k] = nullptr;
+    }
+  if (H->dim == 2) {
+    cudaFree(H->inst2_d);
+    cudaFree(H->items_d);
+    cudaFree(H->ctr_d);
+    H->inst2_d = nullptr;
+    H->items_d = nullptr;
+    H->ctr_d = nullptr;
+    return H->esz == 4 ? setup_2d_t<float>(H) : setup_2d_t<double>(H);
+  }
+  return SP_OK;
+}
+
+int sp_set_stream(sp_handle* H, void* stream) {
+  if (!H) return SP_EINVAL;
+  SP_CUDA(H, cudaStreamSynchronize(H->stream));
+  if (H->own_stream) cudaStreamDestroy(H->stream);
+  H->stream = static_cast<cudaStream_t>(stream);
+  H->own_stream = false;
+  H->graphs = true;
+  for (int k = 0; k < 2; ++k)
+    if (H->gexec[k]) {
+      cudaGraphExecDestroy(H->gexec[k]);
+      H->gexec[k] = nullptr;
+    }
+  return SP_OK;
+}
+
+int sp_synchronize(sp_handle* H) {
+  if (!H) return SP_EINVAL;
+  return check_err_flag(H);
+}
+
+long long sp_launch_count(const sp_handle* H) { return H ? H->launches : -1; }
+
+int sp_field_geometry(const sp_handle* H, int inst, int field, void** dev_origin,
+                      long long* pitch, long long* plane, int halo[3]) {
+  if (!H) return SP_EINVAL;
+  sp_handle* M = const_cast<sp_handle*>(H);
+  if (inst < 0 || inst >= H->batch || field < 0 || field >= H->nf)
+    return fail(M, SP_EINVAL, "instance or field index out of range");
+  if (dev_origin) *dev_origin = field_origin(M, H->cur, inst, field);
+  if (pitch) *pitch = H->pitch;
+  if (plane) *plane = H->plane;
+  if (halo)
+    for (int a = 0; a < 3; ++a) halo[a] = H->h[a];
+  return SP_OK;
+}
+
+const char* sp_last_error(const sp_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+void sp_destroy(sp_handle* h) { release(h); }
+
+}  // extern "C"

@@ -1,0 +1,127 @@
+/*
+ * sp_launch.cuh -- turns a model factory into a registered kernel entry.
+ */
+#pragma once
+
+#include "sp_kernels.cuh"
+#include "sp_models.cuh"
+#include "sp_registry.h"
+
+namespace sp {
+
+template <class MF>
+using model_of = decltype(MF{}());
+
+template <class MF, class T, int LP, int GP, int BP, class TC>
+struct Entry3 {
+  using M = model_of<MF>;
+  using K = Fd3<M, T, LP, GP, BP, TC>;
+  static cudaError_t launch(const void* prm, dim3 grid, cudaStream_t s) {
+    auto kern = k_fd3d<M, T, LP, GP, BP, TC>;
+    static cudaError_t attr = cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
+    if (attr != cudaSuccess) return attr;
+    const M m = MF{}();
+    kern<<<grid, K::NT, K::SMEM, s>>>(*static_cast<const StepParams<T>*>(prm), m);
+    return cudaGetLastError();
+  }
+  static int occupancy() {
+    auto kern = k_fd3d<M, T, LP, GP, BP, TC>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, K::NT, K::SMEM) != cudaSuccess)
+      return 1;
+    return n > 0 ? n : 1;
+  }
+  static KernelInfo info() {
+    return KernelInfo{K::NF, K::NS, K::R, K::HXA, K::TX, K::TY, K::NT, K::SMEM, &launch, &occupancy};
+  }
+};
+
+template <class MF0, class MF1, class T, int LP, int GP, int BP, class TC>
+struct Entry2 {
+  using M0 = model_of<MF0>;
+  using M1 = model_of<MF1>;
+  using K = Fd2<M0, M1, T, LP, GP, BP, TC>;
+  static cudaError_t launch(const void* prm, dim3 grid, cudaStream_t s) {
+    auto kern = k_fd2d<M0, M1, T, LP, GP, BP, TC>;
+    static cudaError_t attr = cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
+    if (attr != cudaSuccess) return attr;
+    const M0 m0 = MF0{}();
+    const M1 m1 = MF1{}();
+    kern<<<grid, K::NT, K::SMEM, s>>>(*static_cast<const Step2Params<T>*>(prm), m0, m1);
+    return cudaGetLastError();
+  }
+  static int occupancy() {
+    auto kern = k_fd2d<M0, M1, T, LP, GP, BP, TC>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, K::NT, K::SMEM) != cudaSuccess)
+      return 1;
+    return n > 0 ? n : 1;
+  }
+  static KernelInfo info() {
+    return KernelInfo{K::NF, K::NS, K::R, K::HXA, K::TX, K::TY, K::NT, K::SMEM, &launch, &occupancy};
+  }
+};
+
+// model factories
+#define SP_FACTORY(NAME, EXPR)                          \
+  struct NAME {                                         \
+    constexpr auto operator()() const { return EXPR; } \
+  };
+SP_FACTORY(MF_A_exact, models::a_exact())
+SP_FACTORY(MF_A_fused, models::a_fused())
+SP_FACTORY(MF_B_exact, models::b_exact())
+SP_FACTORY(MF_B_fused, models::b_fused())
+SP_FACTORY(MF_C_exact, models::c_exact())
+SP_FACTORY(MF_C_fused, models::c_fused())
+SP_FACTORY(MF_AMK_exact, models::amk_exact())
+SP_FACTORY(MF_AMK_fused, models::amk_fused())
+SP_FACTORY(MF_BMK_exact, models::bmk_exact())
+SP_FACTORY(MF_BMK_fused, models::bmk_fused())
+SP_FACTORY(MF_OP_LAP, models::op_lap())
+SP_FACTORY(MF_OP_BILAP, models::op_bilap())
+SP_FACTORY(MF_OP_GRADLAP, models::op_gradlap())
+SP_FACTORY(MF_OP_LAPCUBE, models::op_lapcube())
+#undef SP_FACTORY
+
+}  // namespace sp
+
+// model ids and forms, as in include/symphas_b200.h
+#define SPK_A 0
+#define SPK_B 1
+#define SPK_C 2
+#define SPK_AMK 3
+#define SPK_BMK 4
+#define SPK_ENS_AB 5 /* 2D ensemble: instances of AMK and BMK in one launch */
+#define SPK_OP_LAP 10
+#define SPK_OP_BILAP 11
+#define SPK_OP_GRADLAP 12
+#define SPK_OP_LAPCUBE 13
+#define SPK_EXACT 1
+#define SPK_FUSED 0
+
+// default tiles: 3D (TX, TY, rows per thread, planes in flight), 2D (.., tiles in flight)
+namespace sp {
+template <class T> struct Tiles;
+template <> struct Tiles<float> {
+  using D3 = TileCfg<64, 16, 4, 4>;
+  using D2 = TileCfg<128, 16, 4, 3>;
+};
+template <> struct Tiles<double> {
+  using D3 = TileCfg<64, 8, 2, 4>;
+  using D2 = TileCfg<64, 16, 4, 3>;
+};
+}  // namespace sp
+
+#define SP_REG3(MODEL, FORM, MF, T, DT, LP, GP, BP)                        \
+  ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 3, DT, LP, GP, BP},    \
+                        ::sp::Entry3<::sp::MF, T, LP, GP, BP, ::sp::Tiles<T>::D3>::info())
+#define SP_REG2(MODEL, FORM, MF, T, DT, LP, GP, BP)                        \
+  ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 2, DT, LP, GP, BP},    \
+                        ::sp::Entry2<::sp::MF, ::sp::MF, T, LP, GP, BP, ::sp::Tiles<T>::D2>::info())
+#define SP_REG2X(MODEL, FORM, MF0, MF1, T, DT, LP, GP, BP)                 \
+  ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 2, DT, LP, GP, BP},    \
+                        ::sp::Entry2<::sp::MF0, ::sp::MF1, T, LP, GP, BP, ::sp::Tiles<T>::D2>::info())

@@ -1,0 +1,265 @@
+"""Python mirror of SymPhas's model / solver / find_solution surface for the
+explicit finite-difference path, running on the B200 library.
+
+    SymPhas (C++)                                         here
+    ---------------------------------------------------   ---------------------------------
+    SolverFT<Stencil2d2h<5,6,13>>                         SolverFT(Stencil2d2h(5, 6, 13))
+    BoundaryType::PERIODIC || 64_h / 0.5_dh (x, y)        ProblemParameters((64, 64), h=0.5)
+    model_MA_t<2, SolverFT<...>> m{coeff, n, params}      model_MA_t(2, solver, params, coeff)
+    symphas::find_solution(m, dt, steps)                  find_solution(m, dt, steps)
+    m.update(t); m.equation(); m.step(dt)                 same names (equation/update fold
+                                                          into the fused step kernel)
+    m.system<0>().values / get_field<0>()                 m.get_field(0)
+
+References (paths inside the SymPhas tree): MODEL macros
+sol/inc/modelmacros.h:597-626; Model constructors sol/inc/model.h:100-128;
+find_solution modules-io.h:747-753 and modules-none.h:42-54; model_iteration
+modules-models.h:435-467; Stencil2d2h/Stencil3d2h sol/inc/stencilincludes.h:315-409
+(defaults <9,6,13> and <15,10,25>, :758-792 and :884-921).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi as C
+
+
+class Stencil2d2h:
+    """Stencil2d2h<L, G, B>: laplacian, gradlaplacian and bilaplacian point counts."""
+
+    dim = 2
+
+    def __init__(self, L=9, G=6, B=13):
+        self.points = (int(L), int(G), int(B))
+
+
+class Stencil3d2h:
+    """Stencil3d2h<L, G, B>."""
+
+    dim = 3
+
+    def __init__(self, L=15, G=10, B=25):
+        self.points = (int(L), int(G), int(B))
+
+
+class SolverFT:
+    """Forward-Euler finite-difference solver (examples/solvers/solverft.h).
+
+    form="exact" evaluates the printed scheme term by term without FMA, which
+    is bit-identical to the CPU solver in FP64; form="fused" uses the
+    algebraically equal fused form (fewer operations, rounding differs)."""
+
+    def __init__(self, stencil, form="fused"):
+        if form not in ("exact", "fused"):
+            raise ValueError("form must be 'exact' or 'fused'")
+        self.stencil = stencil
+        self.form = form
+
+
+class BoundaryType:
+    PERIODIC = C.SP_PERIODIC
+    DEFAULT = C.SP_DIRICHLET  # with BoundaryTag::CONSTANT
+
+
+class ProblemParameters:
+    """Grid extents (interior points per axis, x first), uniform spacing h and
+    one boundary per side (LEFT RIGHT TOP BOTTOM FRONT BACK).  A single
+    boundary value applies to every side."""
+
+    def __init__(self, dims, h=1.0, boundary=BoundaryType.PERIODIC, boundary_value=0.0):
+        self.dims = tuple(int(x) for x in dims)
+        self.h = float(h)
+        self.boundary = list(boundary) if isinstance(boundary, (list, tuple)) else [boundary] * 6
+        bv = boundary_value
+        self.boundary_value = list(bv) if isinstance(bv, (list, tuple)) else [float(bv)] * 6
+
+
+_DTYPES = {"f32": (C.SP_F32, np.float32), "f64": (C.SP_F64, np.float64)}
+
+
+class Model:
+    """A device-resident model: fields live in HBM between steps and are read
+    back only by get_field / reduce."""
+
+    model_id = None
+    nfields = 1
+
+    def __init__(self, dim, solver, params, coeff=(), dtype="f64", batch=1, dt=0.0):
+        if self.model_id is None:
+            raise TypeError("use one of the model_*_t classes")
+        if solver.stencil.dim != dim or len(params.dims) != dim:
+            raise ValueError("dimension of the model, stencil and problem parameters differ")
+        if dtype not in _DTYPES:
+            raise ValueError("dtype must be 'f32' or 'f64'")
+        self.dim = dim
+        self.dims = params.dims
+        self.dtype_code, self.np_dtype = _DTYPES[dtype]
+        d = C.SpDesc()
+        d.dim = dim
+        for i, v in enumerate(list(params.dims) + [1] * (3 - dim)):
+            d.n[i] = v
+        d.dtype = self.dtype_code
+        d.model = self.model_id
+        d.form = C.SP_FORM_EXACT if solver.form == "exact" else C.SP_FORM_FUSED
+        d.lap_pts, d.gradlap_pts, d.bilap_pts = solver.stencil.points
+        for i in range(6):
+            d.boundary[i] = params.boundary[i]
+            d.boundary_value[i] = params.boundary_value[i]
+        d.h = params.h
+        d.dt = float(dt)
+        cs = list(coeff) + [1.0] * (8 - len(coeff))  # c(i) defaults to 1
+        for i in range(8):
+            d.coeff[i] = float(cs[i])
+        d.ncoeff = len(coeff)
+        d.batch = int(batch)
+        self.desc = d
+        self.batch = int(batch)
+        self._h = C._H()
+        C.check(C.lib().sp_create(ctypes.byref(d), ctypes.byref(self._h)))
+        self.index = 0
+        self.time = 0.0
+        self.dt = float(dt)
+
+    # --- lifetime -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            C.lib().sp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --- fields -------------------------------------------------------------
+    @property
+    def shape(self):
+        return tuple(reversed(self.dims))
+
+    def _nbytes(self):
+        return int(np.prod(self.dims)) * np.dtype(self.np_dtype).itemsize
+
+    def set_field(self, field, values, inst=0):
+        a = np.ascontiguousarray(values, dtype=self.np_dtype)
+        if a.shape != self.shape:
+            raise ValueError("field shape %s != %s" % (a.shape, self.shape))
+        C.check(C.lib().sp_upload(self._h, inst, field, a.ctypes.data, a.nbytes), self._h)
+
+    def fill_uniform(self, field, seed, lo, hi, inst=0):
+        """Seeded SplitMix64 initial values, bit-identical to the oracle."""
+        C.check(C.lib().sp_fill_uniform(self._h, inst, field, seed, lo, hi), self._h)
+
+    def get_field(self, field=0, inst=0):
+        out = np.empty(self.shape, dtype=self.np_dtype)
+        C.check(C.lib().sp_download(self._h, inst, field, out.ctypes.data, out.nbytes), self._h)
+        return out
+
+    def eval_rhs(self, field=0, inst=0):
+        """dframe of the current state (one evaluation of the equations)."""
+        out = np.empty(self.shape, dtype=self.np_dtype)
+        C.check(C.lib().sp_eval_rhs(self._h, inst, field, out.ctypes.data, out.nbytes), self._h)
+        return out
+
+    # --- time stepping (SolverFT) -----------------------------------------------
+    def update(self, t=None):
+        """Halo refresh: done inside every fused step, nothing to do here."""
+
+    def equation(self):
+        """Evaluation of dframe: fused into step()."""
+
+    def step(self, dt, n=1):
+        if dt != self.dt:
+            C.check(C.lib().sp_set_dt(self._h, float(dt)), self._h)
+            self.dt = float(dt)
+        C.check(C.lib().sp_step(self._h, int(n)), self._h)
+        self.index += n
+        self.time += n * dt
+
+    def step_mass(self, dt, n):
+        """n steps; the last one also returns the FP64 mass of field 0 of every
+        instance, reduced inside the step kernel."""
+        if dt != self.dt:
+            C.check(C.lib().sp_set_dt(self._h, float(dt)), self._h)
+            self.dt = float(dt)
+        out = (ctypes.c_double * self.batch)()
+        C.check(C.lib().sp_step_mass(self._h, int(n), out), self._h)
+        self.index += n
+        self.time += n * dt
+        return np.array(out[:])
+
+    def reduce(self, field=0, inst=0):
+        """(mass, free energy) in FP64."""
+        m = ctypes.c_double()
+        e = ctypes.c_double()
+        C.check(C.lib().sp_reduce(self._h, inst, field, ctypes.byref(m), ctypes.byref(e)),
+                self._h)
+        return m.value, e.value
+
+    def synchronize(self):
+        C.check(C.lib().sp_synchronize(self._h), self._h)
+
+    def set_stream(self, stream_ptr):
+        C.check(C.lib().sp_set_stream(self._h, ctypes.c_void_p(stream_ptr)), self._h)
+
+    def launch_count(self):
+        return C.lib().sp_launch_count(self._h)
+
+    def get_index(self):
+        return self.index
+
+    def get_time(self):
+        return self.time
+
+
+class model_MA_t(Model):
+    """MODEL(MA, (SCALAR), EVOLUTION(dpsi = lap(psi) + (c(1) - c(2) psi^2) psi))."""
+
+    model_id = C.SP_MODEL_A
+
+
+class model_MB_t(Model):
+    """MODEL(MB, (SCALAR), EVOLUTION(dpsi = -bilap(psi) - lap((c(1) - c(2) psi^2) psi)))."""
+
+    model_id = C.SP_MODEL_B
+
+
+class model_MC_t(Model):
+    """Model C with coupling gamma = c(1): conserved psi, non-conserved eta."""
+
+    model_id = C.SP_MODEL_C
+    nfields = 2
+
+
+class model_MAMK_t(Model):
+    """dpsi = M (kappa lap(psi) - psi^3 + psi), M = c(1), kappa = c(2)."""
+
+    model_id = C.SP_MODEL_AMK
+
+
+class model_MBMK_t(Model):
+    """dpsi = M lap(psi^3 - psi - kappa lap(psi)), M = c(1), kappa = c(2)."""
+
+    model_id = C.SP_MODEL_BMK
+
+
+class model_OP_t(Model):
+    """Single-operator model dframe = op(psi), to check a stencil point set."""
+
+    def __init__(self, op, dim, solver, params, dtype="f64"):
+        self.model_id = {"lap": C.SP_OP_LAP, "bilap": C.SP_OP_BILAP,
+                         "gradlap": C.SP_OP_GRADLAP, "lapcube": C.SP_OP_LAPCUBE}[op]
+        super().__init__(dim, solver, params, dtype=dtype)
+
+
+def find_solution(model, dt, steps):
+    """symphas::find_solution(model, dt, steps): advance `steps` iterations."""
+    model.update(model.time)
+    model.step(dt, steps)
+    return model

@@ -1,0 +1,222 @@
+"""GPU parity: the fused sm_100a kernels (through the C ABI) against the CPU
+oracle on the same seeded fields.
+
+Tolerances: FP64 exact form -- bit-identical (and therefore <= 1e-12 relative
+L-infinity); FP64 fused form -- 1e-10 relative; FP32 -- stated per case
+against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+import spo
+import symphas_b200 as sp
+
+pytestmark = pytest.mark.gpu
+
+S2 = sp.Stencil2d2h(5, 6, 13)
+S3 = sp.Stencil3d2h(7, 10, 25)
+
+
+def rel_linf(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def oracle_init(seed, lo, hi, shape):
+    return spo.seed_uniform(seed, lo, hi, int(np.prod(shape))).reshape(shape)
+
+
+def model_of(cls, dim, dims, h, form="exact", dtype="f64", stencil=None, coeff=(), **kw):
+    st = stencil or (S2 if dim == 2 else S3)
+    return cls(dim, sp.SolverFT(st, form=form), sp.ProblemParameters(dims, h=h, **kw),
+               coeff=coeff, dtype=dtype)
+
+
+@pytest.mark.parametrize("dim,dims", [(2, (64, 48)), (3, (24, 20, 16))])
+def test_fill_uniform_matches_oracle_bits(dim, dims):
+    m = model_of(sp.model_MA_t, dim, dims, 1.0)
+    m.fill_uniform(0, 1234, -0.3, 0.1)
+    got = m.get_field(0)
+    ref = oracle_init(1234, -0.3, 0.1, m.shape)
+    assert np.array_equal(got, ref)
+    m32 = model_of(sp.model_MA_t, dim, dims, 1.0, dtype="f32")
+    m32.fill_uniform(0, 1234, -0.3, 0.1)
+    assert np.array_equal(m32.get_field(0), ref.astype(np.float32))
+
+
+def test_model_a_2d_config_bit_identical():
+    """Allen-Cahn 64x64 periodic, dx 0.5, dt 0.01, 1000 steps, Stencil2d2h<5,6,13>."""
+    n, h, dt, steps = 64, 0.5, 0.01, 1000
+    m = model_of(sp.model_MA_t, 2, (n, n), h)
+    m.fill_uniform(0, 11, -0.1, 0.1)
+    sp.find_solution(m, dt, steps)
+    got = m.get_field(0)
+    ref = spo.run(spo.make_desc(2, (n, n), spo.MODEL_A, h, dt), oracle_init(11, -0.1, 0.1, (n, n)),
+                  steps)
+    assert rel_linf(got, ref) <= 1e-12
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("mean", [0.0, -0.2])
+def test_model_b_3d_bit_identical(mean):
+    """Cahn-Hilliard 3D, dx 1, dt 0.005, Stencil3d2h<7,10,25>, 32^3, 200 steps."""
+    n, h, dt, steps = 32, 1.0, 0.005, 200
+    m = model_of(sp.model_MB_t, 3, (n, n, n), h)
+    m.fill_uniform(0, 5, mean - 0.1, mean + 0.1)
+    sp.find_solution(m, dt, steps)
+    got = m.get_field(0)
+    ref = spo.run(spo.make_desc(3, (n, n, n), spo.MODEL_B, h, dt),
+                  oracle_init(5, mean - 0.1, mean + 0.1, (n, n, n)), steps)
+    assert rel_linf(got, ref) <= 1e-12
+    assert np.array_equal(got, ref)
+
+
+OPS2 = [("lap", (5, 6, 13)), ("lap", (9, 6, 13)), ("bilap", (5, 6, 13)), ("bilap", (5, 6, 17)),
+        ("bilap", (5, 6, 21)), ("gradlap", (5, 6, 13)), ("gradlap", (5, 8, 13)),
+        ("gradlap", (5, 12, 13)), ("gradlap", (5, 16, 13)), ("lapcube", (5, 6, 13))]
+OPS3 = [("lap", (7, 10, 25)), ("lap", (15, 10, 25)), ("lap", (19, 10, 25)), ("lap", (21, 10, 25)),
+        ("lap", (27, 10, 25)), ("bilap", (7, 10, 21)), ("bilap", (7, 10, 25)),
+        ("bilap", (7, 10, 41)), ("bilap", (7, 10, 52)), ("bilap", (7, 10, 57)),
+        ("gradlap", (7, 10, 25)), ("gradlap", (7, 12, 25)), ("gradlap", (7, 28, 25)),
+        ("gradlap", (7, 36, 25)), ("gradlap", (7, 40, 25)), ("lapcube", (7, 10, 25))]
+OPID = {"lap": spo.OP_LAP, "bilap": spo.OP_BILAP, "gradlap": spo.OP_GRADLAP,
+        "lapcube": spo.OP_LAPCUBE}
+
+
+@pytest.mark.parametrize("op,pts", OPS2)
+def test_operator_2d_every_point_set(op, pts):
+    dims, h = (40, 36), 0.7
+    st = sp.Stencil2d2h(*pts)
+    m = sp.model_OP_t(op, 2, sp.SolverFT(st, form="exact"), sp.ProblemParameters(dims, h=h))
+    m.fill_uniform(0, 99, -1.0, 1.0)
+    got = m.eval_rhs(0)
+    x = oracle_init(99, -1.0, 1.0, m.shape)
+    ref = spo.rhs(spo.make_desc(2, dims, OPID[op], h, 0.0, stencil=pts), x)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("op,pts", OPS3)
+def test_operator_3d_every_point_set(op, pts):
+    dims, h = (20, 18, 16), 0.9
+    st = sp.Stencil3d2h(*pts)
+    m = sp.model_OP_t(op, 3, sp.SolverFT(st, form="exact"), sp.ProblemParameters(dims, h=h))
+    m.fill_uniform(0, 77, -1.0, 1.0)
+    got = m.eval_rhs(0)
+    x = oracle_init(77, -1.0, 1.0, m.shape)
+    ref = spo.rhs(spo.make_desc(3, dims, OPID[op], h, 0.0, stencil=pts), x)
+    assert np.array_equal(got, ref)
+
+
+def test_model_c_3d_bit_identical():
+    n, h, dt, steps, gamma = 16, 1.0, 0.005, 60, 0.5
+    m = model_of(sp.model_MC_t, 3, (n, n, n), h, coeff=(gamma,))
+    m.fill_uniform(0, 1, 0.0, 0.2)
+    m.fill_uniform(1, 2, -0.1, 0.1)
+    sp.find_solution(m, dt, steps)
+    got = np.stack([m.get_field(0), m.get_field(1)])
+    x = np.stack([oracle_init(1, 0.0, 0.2, (n, n, n)), oracle_init(2, -0.1, 0.1, (n, n, n))])
+    ref = spo.run(spo.make_desc(3, (n, n, n), spo.MODEL_C, h, dt, coeff=(gamma,)), x, steps)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("cls,oid", [(sp.model_MAMK_t, spo.MODEL_AMK), (sp.model_MBMK_t, spo.MODEL_BMK)])
+def test_mobility_kappa_models_2d_bit_identical(cls, oid):
+    dims, h, dt, steps, coeff = (48, 40), 1.0, 0.01, 150, (1.3, 0.7)
+    m = model_of(cls, 2, dims, h, coeff=coeff)
+    m.fill_uniform(0, 3, -0.1, 0.1)
+    sp.find_solution(m, dt, steps)
+    ref = spo.run(spo.make_desc(2, dims, oid, h, dt, coeff=coeff), oracle_init(3, -0.1, 0.1, m.shape),
+                  steps)
+    assert np.array_equal(m.get_field(0), ref)
+
+
+@pytest.mark.parametrize("dim,dims", [(2, (37, 45)), (3, (21, 13, 11))])
+def test_ragged_sizes_bit_identical(dim, dims):
+    h, dt, steps = 1.0, 0.002, 40
+    m = model_of(sp.model_MB_t, dim, dims, h)
+    m.fill_uniform(0, 8, -0.3, 0.3)
+    sp.find_solution(m, dt, steps)
+    ref = spo.run(spo.make_desc(dim, dims, spo.MODEL_B, h, dt), oracle_init(8, -0.3, 0.3, m.shape),
+                  steps)
+    assert np.array_equal(m.get_field(0), ref)
+
+
+@pytest.mark.parametrize("dim,dims,cls,oid", [(2, (40, 32), sp.model_MA_t, spo.MODEL_A),
+                                              (3, (16, 16, 12), sp.model_MB_t, spo.MODEL_B)])
+def test_dirichlet_bit_identical(dim, dims, cls, oid):
+    h, dt, steps, val = 1.0, 0.004, 50, 0.3
+    m = model_of(cls, dim, dims, h, boundary=sp.BoundaryType.DEFAULT, boundary_value=val)
+    m.fill_uniform(0, 4, -0.5, 0.5)
+    sp.find_solution(m, dt, steps)
+    ref = spo.run(spo.make_desc(dim, dims, oid, h, dt, bc=spo.DIRICHLET, bcv=val),
+                  oracle_init(4, -0.5, 0.5, m.shape), steps)
+    assert np.array_equal(m.get_field(0), ref)
+
+
+def test_fused_f64_close_to_oracle():
+    n, h, dt, steps = 32, 1.0, 0.005, 200
+    m = model_of(sp.model_MB_t, 3, (n, n, n), h, form="fused")
+    m.fill_uniform(0, 5, -0.3, -0.1)
+    sp.find_solution(m, dt, steps)
+    ref = spo.run(spo.make_desc(3, (n, n, n), spo.MODEL_B, h, dt), oracle_init(5, -0.3, -0.1, m.shape),
+                  steps)
+    assert rel_linf(m.get_field(0), ref) <= 1e-10
+
+
+@pytest.mark.parametrize("dim,dims,cls,oid,h,dt,steps,tol", [
+    (2, (64, 64), sp.model_MA_t, spo.MODEL_A, 0.5, 0.01, 1000, 1e-4),
+    (3, (32, 32, 32), sp.model_MB_t, spo.MODEL_B, 1.0, 0.005, 200, 1e-5),
+])
+def test_f32_fused_against_f64_oracle(dim, dims, cls, oid, h, dt, steps, tol):
+    m = model_of(cls, dim, dims, h, form="fused", dtype="f32")
+    m.fill_uniform(0, 21, -0.3, -0.1)
+    sp.find_solution(m, dt, steps)
+    ref = spo.run(spo.make_desc(dim, dims, oid, h, dt), oracle_init(21, -0.3, -0.1, m.shape), steps)
+    assert rel_linf(m.get_field(0).astype(np.float64), ref) <= tol
+
+
+def test_batch_instances_match_single_runs():
+    n, dt, steps = 16, 0.005, 30
+    params = sp.ProblemParameters((n, n, n), h=1.0)
+    mb = sp.model_MB_t(3, sp.SolverFT(S3, form="exact"), params, batch=3)
+    for i in range(3):
+        mb.fill_uniform(0, 100 + i, -0.2, 0.2, inst=i)
+    sp.find_solution(mb, dt, steps)
+    for i in range(3):
+        ref = spo.run(spo.make_desc(3, (n, n, n), spo.MODEL_B, 1.0, dt),
+                      oracle_init(100 + i, -0.2, 0.2, (n, n, n)), steps)
+        assert np.array_equal(mb.get_field(0, inst=i), ref)
+
+
+def test_graph_replay_equals_direct_launches():
+    n, dt = 24, 0.005
+    a = model_of(sp.model_MB_t, 3, (n, n, n), 1.0, form="fused", dtype="f32")
+    b = model_of(sp.model_MB_t, 3, (n, n, n), 1.0, form="fused", dtype="f32")
+    for m in (a, b):
+        m.fill_uniform(0, 9, -0.2, 0.2)
+    a.step(dt, 70)  # 2 graph replays of 32 steps + 6 launches
+    for _ in range(70):
+        b.step(dt, 1)
+    assert np.array_equal(a.get_field(0), b.get_field(0))
+    assert a.launch_count() == 70 and b.launch_count() == 70
+
+
+def test_mass_conservation_and_fused_reduction():
+    n, dt = 48, 0.005
+    m = model_of(sp.model_MB_t, 3, (n, n, n), 1.0, form="fused", dtype="f64")
+    m.fill_uniform(0, 13, -0.3, -0.1)
+    m0, e0 = m.reduce(0)
+    masses = m.step_mass(dt, 500)
+    m1, e1 = m.reduce(0)
+    assert abs(m1 - m0) <= 1e-10 * abs(m0)
+    assert abs(masses[0] - m1) <= 1e-12 * abs(m1)
+    assert e1 < e0  # Cahn-Hilliard free energy decreases
+
+
+def test_f32_mass_drift_with_fp64_reduction():
+    n, dt = 64, 0.005
+    m = model_of(sp.model_MB_t, 3, (n, n, n), 1.0, form="fused", dtype="f32")
+    m.fill_uniform(0, 13, -0.3, -0.1)
+    m0, _ = m.reduce(0)
+    m.step(dt, 1000)
+    m1, _ = m.reduce(0)
+    assert abs(m1 - m0) <= 1e-4 * abs(m0)
