@@ -32,7 +32,7 @@
  * results, the manufactured-solution convergence example of SymPhas,
  * conservation) rather than by outputs of SymPhas itself: parity unpinned.
  *
- * Build: oracle/Makefile (gcc -O2 -ffp-contract=off -fopenmp -shared).
+ * Build: oracle/Makefile (gcc -O3 -ffp-contract=off -fopenmp -shared).
  * Floating-point contraction is disabled so every product and sum rounds on
  * its own, as in the reference's plain C++ expression evaluation.
  */
@@ -119,40 +119,47 @@ static spo_geom spo_make_geom(const spo_desc* d) {
 /* Fill the halo.  A halo cell outside the domain along a DIRICHLET axis takes
  * that side's value (later sides in LEFT..BACK order win); a cell outside only
  * along periodic axes takes the value of its periodic image. */
+static void spo_halo_cell(const spo_desc* d, const spo_geom* g, double* v, long i, long j,
+                          long k) {
+  const int D = d->dim;
+  long c[3] = {i - BD, j - BD, (D == 3) ? k - BD : 0};
+  int dir = -1;
+  double dval = 0;
+  for (int a = 0; a < D; ++a) {
+    if (c[a] < 0 && d->bc[2 * a] == SPO_DIRICHLET) { dir = 2 * a; dval = d->bcv[2 * a]; }
+    if (c[a] >= d->n[a] && d->bc[2 * a + 1] == SPO_DIRICHLET) { dir = 2 * a + 1; dval = d->bcv[2 * a + 1]; }
+  }
+  long idx = i + j * g->s[1] + k * g->s[2];
+  if (dir >= 0) {
+    v[idx] = dval;
+    return;
+  }
+  long w[3];
+  for (int a = 0; a < 3; ++a) {
+    long n = (a < D) ? d->n[a] : 1;
+    long x = c[a];
+    if (a < D) {
+      while (x < 0) x += n;
+      while (x >= n) x -= n;
+    }
+    w[a] = x + ((a < D) ? BD : 0);
+  }
+  v[idx] = v[w[0] + w[1] * g->s[1] + w[2] * g->s[2]];
+}
+
 static void spo_update_halo(const spo_desc* d, const spo_geom* g, double* v) {
   const int D = d->dim;
-  const long kz0 = (D == 3) ? 0 : 0, kz1 = g->L[2];
-  for (long k = kz0; k < kz1; ++k)
-    for (long j = 0; j < g->L[1]; ++j)
-      for (long i = 0; i < g->L[0]; ++i) {
-        long c[3] = {i - BD, j - BD, (D == 3) ? k - BD : 0};
-        int outside = 0;
-        for (int a = 0; a < D; ++a)
-          if (c[a] < 0 || c[a] >= d->n[a]) outside = 1;
-        if (!outside) continue;
-        int dir = -1;
-        double dval = 0;
-        for (int a = 0; a < D; ++a) {
-          if (c[a] < 0 && d->bc[2 * a] == SPO_DIRICHLET) { dir = 2 * a; dval = d->bcv[2 * a]; }
-          if (c[a] >= d->n[a] && d->bc[2 * a + 1] == SPO_DIRICHLET) { dir = 2 * a + 1; dval = d->bcv[2 * a + 1]; }
-        }
-        long idx = i + j * g->s[1] + k * g->s[2];
-        if (dir >= 0) {
-          v[idx] = dval;
-          continue;
-        }
-        long w[3];
-        for (int a = 0; a < 3; ++a) {
-          long n = (a < D) ? d->n[a] : 1;
-          long x = c[a];
-          if (a < D) {
-            while (x < 0) x += n;
-            while (x >= n) x -= n;
-          }
-          w[a] = x + ((a < D) ? BD : 0);
-        }
-        v[idx] = v[w[0] + w[1] * g->s[1] + w[2] * g->s[2]];
+  for (long k = 0; k < g->L[2]; ++k)
+    for (long j = 0; j < g->L[1]; ++j) {
+      int row_out = (j < BD || j >= BD + d->n[1]) ||
+                    (D == 3 && (k < BD || k >= BD + d->n[2]));
+      if (row_out) {
+        for (long i = 0; i < g->L[0]; ++i) spo_halo_cell(d, g, v, i, j, k);
+      } else {
+        for (long i = 0; i < BD; ++i) spo_halo_cell(d, g, v, i, j, k);
+        for (long i = BD + d->n[0]; i < g->L[0]; ++i) spo_halo_cell(d, g, v, i, j, k);
       }
+    }
 }
 
 /* ------------------------------------------------------------------ */
@@ -592,6 +599,25 @@ static void spo_copy_out(const spo_sys* s, double* const* src, int f, double* in
 /* ------------------------------------------------------------------ */
 
 int spo_fields(int model) { return spo_field_count(model); }
+
+/* A persistent system, for timing loops: create, upload, step, download. */
+void* spo_create(const spo_desc* d, int threads) {
+  spo_sys* s = (spo_sys*)malloc(sizeof(spo_sys));
+  spo_sys_init(s, d, threads);
+  return s;
+}
+void spo_set(void* h, int f, const double* interior) { spo_copy_in((spo_sys*)h, f, interior); }
+void spo_get(void* h, int f, double* interior) {
+  spo_sys* s = (spo_sys*)h;
+  spo_copy_out(s, s->psi, f, interior);
+}
+void spo_step(void* h, int nsteps) {
+  for (int i = 0; i < nsteps; ++i) spo_sys_step((spo_sys*)h);
+}
+void spo_destroy(void* h) {
+  spo_sys_free((spo_sys*)h);
+  free(h);
+}
 
 /* Advance `fields` (nf interior arrays laid out back to back, x-fastest) by
  * `nsteps` SolverFT iterations using `threads` OpenMP threads.  Returns 0. */

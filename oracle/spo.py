@@ -48,6 +48,12 @@ def _load():
     lib.spo_run_batch.argtypes = [ctypes.POINTER(Desc), ctypes.POINTER(dp), ctypes.c_int,
                                   ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     lib.spo_omp_max_threads.restype = ctypes.c_int
+    lib.spo_create.argtypes = [ctypes.POINTER(Desc), ctypes.c_int]
+    lib.spo_create.restype = ctypes.c_void_p
+    lib.spo_set.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+    lib.spo_get.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+    lib.spo_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.spo_destroy.argtypes = [ctypes.c_void_p]
     return lib
 
 
@@ -120,3 +126,32 @@ def run_batch(descs, fields_list, steps_list, threads):
 
 def max_threads():
     return _lib.spo_omp_max_threads()
+
+
+class System:
+    """A persistent oracle system (no per-call allocation), for timing loops."""
+
+    def __init__(self, d, fields, threads=1):
+        self.d = d
+        self.h = _lib.spo_create(ctypes.byref(d), int(threads))
+        a = np.ascontiguousarray(fields, dtype=np.float64)
+        nf = nfields(d.model)
+        a = a.reshape((nf,) + shape_of(d))
+        for f in range(nf):
+            _lib.spo_set(self.h, f, _ptr(np.ascontiguousarray(a[f])))
+
+    def step(self, n=1):
+        _lib.spo_step(self.h, int(n))
+
+    def get(self, f=0):
+        out = np.empty(shape_of(self.d), dtype=np.float64)
+        _lib.spo_get(self.h, f, _ptr(out))
+        return out
+
+    def close(self):
+        if self.h:
+            _lib.spo_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/symphas_b200.h"
+#include "sp_aux.cuh"
 #include "sp_kernels.cuh"
 #include "sp_registry.h"
 
@@ -444,13 +445,13 @@ int create(const sp_desc* desc, sp_handle* H) {
 
   size_t partial_n = 2 * size_t(H->sms) * 8;
   if (H->dim == 3) {
-    // z planes per CTA: aim for at least ~4 waves of resident CTAs, but keep
-    // chunks long enough that the 2R prologue planes stay a small overhead
+    // z planes per CTA: as many z chunks as fit one wave of resident CTAs
+    // (each chunk re-reads 2R planes, so longer chunks waste less)
     const int occ = H->ki->occupancy();
     const long long tiles = (long long)H->ntx * H->nty * H->batch;
-    const long long want = 4LL * H->sms * occ;
-    int chunks = int((want + tiles - 1) / tiles);
-    chunks = std::max(1, std::min(chunks, std::max(1, H->n[2] / std::max(8, 4 * R))));
+    const long long slots = (long long)H->sms * occ;
+    int chunks = int(std::max(1LL, slots / tiles));
+    chunks = std::min(chunks, std::max(1, H->n[2] / std::max(4, 2 * R)));
     H->zchunk = (H->n[2] + chunks - 1) / chunks;
     if (const char* zc = getenv("SP_ZCHUNK")) {
       const int v = atoi(zc);

@@ -1,0 +1,142 @@
+/*
+ * sp_aux.cuh -- auxiliary kernels around the fused step: halo fill after an
+ * upload, FP64 mass/energy reductions and the deterministic finishing sum.
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "sp_common.cuh"
+
+namespace sp {
+
+// ---------------------------------------------------------------------------
+// halo fill (after an upload): Dirichlet sides take their constant, the rest
+// of the halo takes periodic images -- the same rule as the oracle
+// ---------------------------------------------------------------------------
+template <class T>
+struct HaloParams {
+  T* org;
+  int dim;
+  int n[3], h[3];
+  long long pitch, plane;
+  int bc[6];
+  T bv[6];
+};
+
+template <class T>
+__global__ void k_fill_halo(const HaloParams<T> p) {
+  const long long L0 = p.n[0] + 2 * p.h[0], L1 = p.n[1] + 2 * p.h[1];
+  const long long L2 = (p.dim == 3) ? p.n[2] + 2 * p.h[2] : 1;
+  const long long total = L0 * L1 * L2;
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+       id += (long long)gridDim.x * blockDim.x) {
+    const long long i = id % L0, j = (id / L0) % L1, k = id / (L0 * L1);
+    long long c[3] = {i - p.h[0], j - p.h[1], (p.dim == 3) ? k - p.h[2] : 0};
+    bool outside = false;
+    for (int a = 0; a < p.dim; ++a)
+      if (c[a] < 0 || c[a] >= p.n[a]) outside = true;
+    if (!outside) continue;
+    int dir = -1;
+    T dval = T(0);
+    for (int a = 0; a < p.dim; ++a) {
+      if (c[a] < 0 && p.bc[2 * a] == 1) {
+        dir = 2 * a;
+        dval = p.bv[2 * a];
+      }
+      if (c[a] >= p.n[a] && p.bc[2 * a + 1] == 1) {
+        dir = 2 * a + 1;
+        dval = p.bv[2 * a + 1];
+      }
+    }
+    const long long idx = k * p.plane + j * p.pitch + i;
+    if (dir >= 0) {
+      p.org[idx] = dval;
+      continue;
+    }
+    long long w[3] = {0, 0, 0};
+    for (int a = 0; a < p.dim; ++a) {
+      long long v = c[a] % p.n[a];
+      if (v < 0) v += p.n[a];
+      w[a] = v + p.h[a];
+    }
+    p.org[idx] = p.org[w[2] * p.plane + w[1] * p.pitch + w[0]];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 reductions: mass of one field and the free energy of the system
+// ---------------------------------------------------------------------------
+template <class T>
+struct ReduceParams {
+  const T* f0;  // field whose mass is summed
+  const T* e0;  // fields of the energy (e1 may be null)
+  const T* e1;
+  int dim;
+  int n[3], h[3];
+  long long pitch, plane;
+  int energy_kind;  // 0 Landau(c1,c2), 1 Landau with kappa, 2 model C
+  double c1, c2, kappa, gamma, h_sp;
+  double* partial;  // [2 * gridDim.x]
+};
+
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) k_reduce(const ReduceParams<T> p) {
+  __shared__ double red[32];
+  const long long nx = p.n[0], ny = p.n[1], nz = (p.dim == 3) ? p.n[2] : 1;
+  const long long total = nx * ny * nz;
+  const double ih = 1.0 / p.h_sp;
+  double ms = 0.0, es = 0.0;
+  for (long long id = blockIdx.x * (long long)NT + threadIdx.x; id < total;
+       id += (long long)gridDim.x * NT) {
+    const long long i = id % nx, j = (id / nx) % ny, k = id / (nx * ny);
+    const long long o = (k + (p.dim == 3 ? p.h[2] : 0)) * p.plane + (j + p.h[1]) * p.pitch +
+                        (i + p.h[0]);
+    ms += double(p.f0[o]);
+    double e = 0.0;
+    for (int f = 0; f < (p.e1 ? 2 : 1); ++f) {
+      const T* g = f ? p.e1 : p.e0;
+      const double v = double(g[o]);
+      const double gx = (double(g[o + 1]) - v) * ih, gy = (double(g[o + p.pitch]) - v) * ih;
+      double g2 = gx * gx + gy * gy;
+      if (p.dim == 3) {
+        const double gz = (double(g[o + p.plane]) - v) * ih;
+        g2 += gz * gz;
+      }
+      const double v2 = v * v;
+      if (p.energy_kind == 0)
+        e += -0.5 * p.c1 * v2 + 0.25 * p.c2 * v2 * v2 + 0.5 * g2;
+      else
+        e += -0.5 * v2 + 0.25 * v2 * v2 + 0.5 * p.kappa * g2;
+    }
+    if (p.energy_kind == 2 && p.e1) {
+      const double a = double(p.e0[o]), b = double(p.e1[o]);
+      e += p.gamma * a * a * b * b;
+    }
+    es += e;
+  }
+  const double m = block_sum<NT>(ms, red);
+  __syncthreads();
+  const double e = block_sum<NT>(es, red);
+  if (threadIdx.x == 0) {
+    p.partial[2 * blockIdx.x] = m;
+    p.partial[2 * blockIdx.x + 1] = e;
+  }
+}
+
+// sums `count` groups of `stride` partials in a fixed order (deterministic)
+template <int NT>
+__global__ void __launch_bounds__(NT)
+    k_finish(const double* partial, int count, int stride, double* out) {
+  __shared__ double red[32];
+  for (int s = 0; s < stride; ++s) {
+    double v = 0.0;
+    for (int i = threadIdx.x; i < count; i += NT) v += partial[size_t(i) * stride + s];
+    const double t = block_sum<NT>(v, red);
+    if (threadIdx.x == 0) out[s] = t;
+    __syncthreads();
+  }
+}
+
+}  // namespace sp

@@ -1,0 +1,148 @@
+/*
+ * sp_common.cuh -- small device helpers shared by the step and auxiliary
+ * kernels: integer helpers, the W-wide value type of the vectorised
+ * evaluator, the shared-memory evaluation context and block reductions.
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sp {
+
+constexpr int ceil_to(int a, int b) { return (a + b - 1) / b * b; }
+constexpr int imax(int a, int b) { return a > b ? a : b; }
+constexpr int floordiv(int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); }
+
+enum : int { KERR_NONE = 0, KERR_TMA_TIMEOUT = 1 };
+
+// ---------------------------------------------------------------------------
+// Vec<T, W>: W consecutive x-sites evaluated together.  Every operation is
+// elementwise, so an expression evaluated on Vec rounds exactly like W scalar
+// evaluations (the FP64 exact form stays bit-identical to the CPU solver),
+// while shared-memory traffic moves as 8- or 16-byte words.
+// ---------------------------------------------------------------------------
+template <class T, int W>
+struct alignas(sizeof(T) * W) Vec {
+  T v[W];
+  Vec() = default;
+  template <class S>
+  __host__ __device__ __forceinline__ explicit Vec(S s) {
+#pragma unroll
+    for (int j = 0; j < W; ++j) v[j] = T(s);
+  }
+};
+
+#define SP_VEC_BINOP(OP)                                                           \
+  template <class T, int W>                                                        \
+  __device__ __forceinline__ Vec<T, W> operator OP(const Vec<T, W>& a, const Vec<T, W>& b) { \
+    Vec<T, W> r;                                                                   \
+    _Pragma("unroll") for (int j = 0; j < W; ++j) r.v[j] = a.v[j] OP b.v[j];       \
+    return r;                                                                      \
+  }
+SP_VEC_BINOP(+)
+SP_VEC_BINOP(-)
+SP_VEC_BINOP(*)
+#undef SP_VEC_BINOP
+
+template <class T, int W>
+__device__ __forceinline__ Vec<T, W> operator-(const Vec<T, W>& a) {
+  Vec<T, W> r;
+#pragma unroll
+  for (int j = 0; j < W; ++j) r.v[j] = -a.v[j];
+  return r;
+}
+
+template <class T, int W>
+struct VecOf {
+  using type = Vec<T, W>;
+};
+template <class T>
+struct VecOf<T, 1> {
+  using type = T;
+};
+template <class T, int W>
+using vec_t = typename VecOf<T, W>::type;
+
+template <class T>
+__device__ __forceinline__ T lane(const T& x, int) {
+  return x;
+}
+template <class T, int W>
+__device__ __forceinline__ T lane(const Vec<T, W>& x, int j) {
+  return x.v[j];
+}
+template <class T>
+__device__ __forceinline__ void set_lane(T& x, int, T s) {
+  x = s;
+}
+template <class T, int W>
+__device__ __forceinline__ void set_lane(Vec<T, W>& x, int j, T s) {
+  x.v[j] = s;
+}
+
+// value at offset X (elements) from a W-aligned pointer p, as a W-wide vector
+// built from at most two aligned vector loads (offsets are compile-time)
+template <class T, int W, int X>
+__device__ __forceinline__ vec_t<T, W> load_at(const T* p) {
+  if constexpr (W == 1) {
+    return p[X];
+  } else {
+    constexpr int c0 = floordiv(X, W);
+    constexpr int l0 = X - c0 * W;
+    const Vec<T, W> a = *reinterpret_cast<const Vec<T, W>*>(p + c0 * W);
+    if constexpr (l0 == 0) {
+      return a;
+    } else {
+      const Vec<T, W> b = *reinterpret_cast<const Vec<T, W>*>(p + (c0 + 1) * W);
+      Vec<T, W> r;
+#pragma unroll
+      for (int j = 0; j < W; ++j) r.v[j] = (l0 + j < W) ? a.v[l0 + j] : b.v[l0 + j - W];
+      return r;
+    }
+  }
+}
+
+// Evaluation context of one W-wide site group: shared-memory offsets of the
+// field planes (NZ planes centred at ZR) and staged-operand planes, relative
+// to `base`; PW and SW are the row pitches of the field and stage tiles.
+template <class T, int W, int DIM, int LP, int GP, int BP, int NF, int NZ, int ZR, int PW,
+          int NS, int NSZ, int SZR, int SW>
+struct Ctx {
+  using scalar_type = T;
+  using value_type = vec_t<T, W>;
+  static constexpr int dim = DIM, lap_points = LP, gradlap_points = GP, bilap_points = BP;
+  const T* base;
+  int fo[NF][NZ];
+  int so[NS > 0 ? NS : 1][NSZ > 0 ? NSZ : 1];
+  value_type divh2, divh3, divh4;
+  const T* cf;
+  template <int I, int X, int Y, int Z>
+  __device__ __forceinline__ value_type var() const {
+    static_assert(I >= 1 && I <= NF, "field index");
+    static_assert(Z + ZR >= 0 && Z + ZR < NZ, "z reach beyond the loaded planes");
+    static_assert(DIM == 3 || Z == 0, "z offset in 2D");
+    return load_at<T, W, X>(base + fo[I - 1][Z + ZR] + Y * PW);
+  }
+  template <int K, int X, int Y, int Z>
+  __device__ __forceinline__ value_type stg() const {
+    static_assert(K >= 0 && K < NS, "stage index");
+    static_assert(Z + SZR >= 0 && Z + SZR < NSZ, "z reach beyond the staged planes");
+    return load_at<T, W, X>(base + so[K][Z + SZR] + Y * SW);
+  }
+  __device__ __forceinline__ value_type coef(int i) const { return value_type(cf[i - 1]); }
+};
+
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane_id = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane_id == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < NT / 32; ++i) s += red[i];
+  return s;
+}
+
+}  // namespace sp

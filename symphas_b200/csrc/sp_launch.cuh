@@ -107,12 +107,12 @@ SP_FACTORY(MF_OP_LAPCUBE, models::op_lapcube())
 namespace sp {
 template <class T> struct Tiles;
 template <> struct Tiles<float> {
-  using D3 = TileCfg<64, 16, 4, 4>;
-  using D2 = TileCfg<128, 16, 4, 3>;
+  using D3 = TileCfg<64, 16, 2, 4, 2>;
+  using D2 = TileCfg<128, 16, 4, 3, 2>;
 };
 template <> struct Tiles<double> {
-  using D3 = TileCfg<64, 8, 2, 4>;
-  using D2 = TileCfg<64, 16, 4, 3>;
+  using D3 = TileCfg<64, 16, 2, 3, 2>;
+  using D2 = TileCfg<64, 16, 4, 3, 2>;
 };
 }  // namespace sp
 

@@ -49,14 +49,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`: gives up after roughly a second.
+// Bounded wait for phase `parity` of `bar`: try_wait already suspends the
+// thread in hardware for a while; give up after about 2^31 SM cycles (~1 s).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   if (mbar_try_wait(bar, parity)) return true;
-  for (uint32_t i = 0; i < (1u << 22); ++i) {
-    __nanosleep(128);
-    if (mbar_try_wait(bar, parity)) return true;
-  }
-  return false;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > (1LL << 31)) return false;
+  return true;
 }
 
 __device__ __forceinline__ void load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x,

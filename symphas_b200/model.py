@@ -152,6 +152,16 @@ class Model:
             raise ValueError("field shape %s != %s" % (a.shape, self.shape))
         C.check(C.lib().sp_upload(self._h, inst, field, a.ctypes.data, a.nbytes), self._h)
 
+    def upload_from(self, field, host_ptr, nbytes, inst=0):
+        """Upload interior values from a raw host pointer (e.g. pinned memory)."""
+        C.check(C.lib().sp_upload(self._h, inst, field, ctypes.c_void_p(host_ptr), nbytes),
+                self._h)
+
+    def download_to(self, field, host_ptr, nbytes, inst=0):
+        """Download interior values to a raw host pointer and wait for them."""
+        C.check(C.lib().sp_download(self._h, inst, field, ctypes.c_void_p(host_ptr), nbytes),
+                self._h)
+
     def fill_uniform(self, field, seed, lo, hi, inst=0):
         """Seeded SplitMix64 initial values, bit-identical to the oracle."""
         C.check(C.lib().sp_fill_uniform(self._h, inst, field, seed, lo, hi), self._h)

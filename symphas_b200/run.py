@@ -1,0 +1,52 @@
+"""Run a built-in model for a number of fused steps on seeded noise and print
+the time per step.  Used for timing and for profiling single launches:
+
+    python -m symphas_b200.run --model B --dim 3 --n 256 --dtype f32 --steps 8
+
+Steps are launched one at a time (no CUDA graph), so a profiler sees each
+fused-step launch separately.
+"""
+import argparse
+import json
+import time
+
+import symphas_b200 as sp
+
+MODELS = {"A": sp.model_MA_t, "B": sp.model_MB_t, "C": sp.model_MC_t,
+          "AMK": sp.model_MAMK_t, "BMK": sp.model_MBMK_t}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--model", default="B", choices=sorted(MODELS))
+    ap.add_argument("--dim", type=int, default=3, choices=[2, 3])
+    ap.add_argument("--n", type=int, default=256, help="interior points per axis")
+    ap.add_argument("--dtype", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--form", default="fused", choices=["fused", "exact"])
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--dt", type=float, default=0.005)
+    ap.add_argument("--h", type=float, default=1.0)
+    ap.add_argument("--coeff", type=float, nargs="*", default=[])
+    a = ap.parse_args(argv)
+    st = sp.Stencil2d2h(5, 6, 13) if a.dim == 2 else sp.Stencil3d2h(7, 10, 25)
+    cls = MODELS[a.model]
+    coeff = a.coeff or ([0.5] if a.model == "C" else [])
+    m = cls(a.dim, sp.SolverFT(st, form=a.form), sp.ProblemParameters((a.n,) * a.dim, h=a.h),
+            coeff=coeff, dtype=a.dtype)
+    m.fill_uniform(0, 1, -0.3, -0.1)
+    if cls.nfields > 1:
+        m.fill_uniform(1, 2, -0.1, 0.1)
+    m.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        m.step(a.dt, 1)
+    m.synchronize()
+    el = time.perf_counter() - t0
+    print(json.dumps({"model": a.model, "dim": a.dim, "n": a.n, "dtype": a.dtype, "form": a.form,
+                      "steps": a.steps, "wall_ms_per_step": 1e3 * el / a.steps,
+                      "launches": m.launch_count()}))
+    m.close()
+
+
+if __name__ == "__main__":
+    main()
