@@ -146,6 +146,35 @@ long long sp_launch_count(const sp_handle* h);
 int sp_field_geometry(const sp_handle* h, int inst, int field, void** dev_origin,
                       long long* pitch, long long* plane, int halo[3]);
 
+/* ---- no-allocation variant of the reduction -------------------------------
+ * No counterpart in SymPhas.  For callers that cannot call cudaMalloc -- an
+ * application whose device memory belongs to another allocator (a framework's
+ * caching pool that has reserved the GPU, a host with a fixed memory budget),
+ * or a stepping loop that must not stall, as cudaMalloc and cudaFree can
+ * synchronise the whole device.  Same sums as sp_reduce, but on fields the
+ * caller already holds in device memory and without a handle:
+ *   fields  device pointer, `batch` instances back to back, each holding the
+ *           model's fields (2 for SP_MODEL_C, else 1) as compact interiors
+ *           (x-fastest, periodic on every axis), dtype SP_F32 or SP_F64;
+ *   out     device pointer to 2 * batch doubles: (mass of field 0, energy)
+ *           per instance; written in stream order on `stream`;
+ *   model, coeff, h select the free-energy density as in sp_reduce.
+ * It calls no allocator.  Its scratch is one static device array of
+ * SP_NOALLOC_MAX_INSTANCES * SP_NOALLOC_BLOCKS_PER_INSTANCE * 2 doubles
+ * (128 KiB) that every GPU loading this library keeps until the process exits;
+ * batch > SP_NOALLOC_MAX_INSTANCES is rejected with SP_EINVAL.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture.  Every call shares the
+ * array: calls that overlap on the GPU (other streams, other host threads)
+ * race and must be ordered by the caller. */
+#define SP_NOALLOC_MAX_INSTANCES 64
+#define SP_NOALLOC_BLOCKS_PER_INSTANCE 128
+int sp_reduce_fields_noalloc(const void* fields, int dtype, int dim, const int n[3], int model,
+                             const double coeff[8], double h, int batch, double* out,
+                             void* stream);
+/* Message of the last failure of sp_reduce_fields_noalloc on this thread. */
+const char* sp_noalloc_error(void);
+
 const char* sp_last_error(const sp_handle* h);
 /* Message of the last failure of sp_create (no handle exists then). */
 const char* sp_create_error(void);

@@ -17,6 +17,7 @@ SP_PERIODIC, SP_DIRICHLET = 0, 1
 SP_MODEL_A, SP_MODEL_B, SP_MODEL_C, SP_MODEL_AMK, SP_MODEL_BMK = 0, 1, 2, 3, 4
 SP_OP_LAP, SP_OP_BILAP, SP_OP_GRADLAP, SP_OP_LAPCUBE = 10, 11, 12, 13
 SP_FORM_EXACT, SP_FORM_FUSED = 1, 0
+SP_NOALLOC_MAX_INSTANCES = 64
 
 _STATUS = {
     SP_EINVAL: "invalid argument",
@@ -81,6 +82,11 @@ SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_longlong),
                                          ctypes.POINTER(ctypes.c_longlong),
                                          ctypes.POINTER(ctypes.c_int)]),
+    "sp_reduce_fields_noalloc": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                                 ctypes.POINTER(ctypes.c_double), ctypes.c_double,
+                                                 ctypes.c_int, _P, _P]),
+    "sp_noalloc_error": (ctypes.c_char_p, []),
     "sp_last_error": (ctypes.c_char_p, [_H]),
     "sp_create_error": (ctypes.c_char_p, []),
     "sp_destroy": (None, [_H]),
