@@ -131,6 +131,16 @@ int sp_download_device(sp_handle* h, int inst, int field, void* dev, size_t byte
  * (forward-difference gradients).  Waits for the result. */
 int sp_reduce(sp_handle* h, int inst, int field, double* mass, double* energy);
 
+/* Time every tile shape built for this kernel on this GPU (`reps` launches
+ * each, evaluating the right-hand side so the fields are not changed) and keep
+ * the fastest; later sp_create calls with the same kernel and size in the same
+ * process start with it.  No counterpart in SymPhas. */
+int sp_autotune(sp_handle* h, int reps);
+/* The chosen kernel shape: {tile x, tile y, rows per thread, TMA stages in
+ * flight, variant index, number of variants, threads per CTA, z planes per
+ * CTA (3D) or persistent CTAs (2D)}. */
+int sp_kernel_info(const sp_handle* h, int info[8]);
+
 /* Change the time step of further sp_step calls (SolverFT's dt, set by
  * Model::step at sol/inc/model.h:932-936). */
 int sp_set_dt(sp_handle* h, double dt);

@@ -74,6 +74,8 @@ SIGNATURES = {
     "sp_download_device": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _P, _SZ]),
     "sp_reduce": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                  ctypes.POINTER(ctypes.c_double)]),
+    "sp_autotune": (ctypes.c_int, [_H, ctypes.c_int]),
+    "sp_kernel_info": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "sp_set_stream": (ctypes.c_int, [_H, _P]),
     "sp_set_dt": (ctypes.c_int, [_H, ctypes.c_double]),
     "sp_synchronize": (ctypes.c_int, [_H]),

@@ -32,15 +32,17 @@ namespace sp {
 // ---------------------------------------------------------------------------
 namespace {
 using KeyT = std::tuple<int, int, int, int, int, int, int>;
-std::map<KeyT, KernelInfo>& table() {
-  static std::map<KeyT, KernelInfo> t;
+std::map<KeyT, std::vector<KernelInfo>>& table() {
+  static std::map<KeyT, std::vector<KernelInfo>> t;
   return t;
 }
 KeyT tup(const KernelKey& k) { return KeyT{k.model, k.form, k.dim, k.dtype, k.lp, k.gp, k.bp}; }
 }  // namespace
 
-void register_kernel(const KernelKey& key, const KernelInfo& info) { table()[tup(key)] = info; }
-const KernelInfo* find_kernel(const KernelKey& key) {
+void register_kernel(const KernelKey& key, const KernelInfo& info) {
+  table()[tup(key)].push_back(info);
+}
+const std::vector<KernelInfo>* find_kernels(const KernelKey& key) {
   auto it = table().find(tup(key));
   return it == table().end() ? nullptr : &it->second;
 }
@@ -82,7 +84,9 @@ __global__ void k_seed(T* org, int dim, int n0, int n1, int n2, int h0, int h1, 
 // ---------------------------------------------------------------------------
 struct sp_handle {
   sp_desc d{};
-  const sp::KernelInfo* ki = nullptr;
+  const sp::KernelInfo* ki = nullptr;   // the chosen tile variant
+  std::vector<sp::KernelInfo> variants;  // every tile shape built for this kernel
+  int variant = 0;
   int nf = 1, batch = 1, dim = 2;
   int n[3] = {1, 1, 1}, h[3] = {0, 0, 0};
   long long pitch = 0, ly = 0, lz = 1, plane = 0, felems = 0;
@@ -327,6 +331,10 @@ int setup_2d_t(sp_handle* H) {
     q.divh4 = T(divh4);
     for (int c = 0; c < 8; ++c) q.coef[c] = T(H->d.coeff[c]);
   }
+  cudaFree(H->inst2_d);
+  cudaFree(H->items_d);
+  H->inst2_d = nullptr;
+  H->items_d = nullptr;
   SP_CUDA(H, cudaMalloc(&H->inst2_d, sizeof(sp::Inst2<T>) * H->batch));
   SP_CUDA(H, cudaMemcpy(H->inst2_d, ip.data(), sizeof(sp::Inst2<T>) * H->batch,
                         cudaMemcpyHostToDevice));
@@ -340,63 +348,31 @@ int setup_2d_t(sp_handle* H) {
     SP_CUDA(H, cudaMemcpy(H->items_d, items.data(), sizeof(int2) * items.size(),
                           cudaMemcpyHostToDevice));
   }
-  SP_CUDA(H, cudaMalloc(&H->ctr_d, 2 * sizeof(int)));
-  SP_CUDA(H, cudaMemset(H->ctr_d, 0, 2 * sizeof(int)));
+  if (!H->ctr_d) {
+    SP_CUDA(H, cudaMalloc(&H->ctr_d, 2 * sizeof(int)));
+    SP_CUDA(H, cudaMemset(H->ctr_d, 0, 2 * sizeof(int)));
+  }
   const int occ = H->ki->occupancy();
   H->grid2 = std::max(1, std::min(H->sms * occ, H->nitems));
   return SP_OK;
 }
 
-int create(const sp_desc* desc, sp_handle* H) {
-  std::string why;
-  if (int rc = validate(desc, why)) return fail(H, rc, why);
-  sp::register_all_kernels();
-  H->d = *desc;
-  H->dim = desc->dim;
-  H->batch = desc->batch;
-  H->esz = desc->dtype == SP_F32 ? 4 : 8;
-  const sp::KernelKey key{desc->model, desc->form, desc->dim, desc->dtype,
-                          desc->lap_pts, desc->gradlap_pts, desc->bilap_pts};
-  H->ki = sp::find_kernel(key);
-  if (!H->ki) {
-    char b[256];
-    snprintf(b, sizeof b,
-             "no fused kernel built for model %d form %d dim %d dtype %d stencil <%d,%d,%d>",
-             desc->model, desc->form, desc->dim, desc->dtype, desc->lap_pts,
-             desc->gradlap_pts, desc->bilap_pts);
-    return fail(H, SP_EINVAL, b);
-  }
-  H->nf = H->ki->nf;
-  for (int a = 0; a < 3; ++a) H->n[a] = (a < H->dim) ? desc->n[a] : 1;
+// TMA descriptors of every field of both buffers (box = the tile plus its
+// halo), output origins, grid sizing and scratch: everything that depends on
+// the chosen tile shape.
+int configure(sp_handle* H, int variant) {
+  SP_CUDA(H, cudaStreamSynchronize(H->stream));
+  H->variant = variant;
+  H->ki = &H->variants[variant];
   const int R = H->ki->R;
-  for (int a = 0; a < H->dim; ++a)
-    if (H->n[a] < 2 * R) return fail(H, SP_EINVAL, "an extent is smaller than twice the stencil reach");
-  H->h[0] = H->ki->hx;
-  H->h[1] = R;
-  H->h[2] = H->dim == 3 ? R : 0;
-  const int va = int(16 / H->esz);
-  H->pitch = ((H->n[0] + 2 * H->h[0] + va - 1) / va) * va;
-  H->ly = H->n[1] + 2 * H->h[1];
-  H->lz = H->dim == 3 ? H->n[2] + 2 * H->h[2] : 1;
-  H->plane = H->pitch * H->ly;
-  H->felems = ((H->plane * H->lz + 63) / 64) * 64;
   H->ntx = (H->n[0] + H->ki->tx - 1) / H->ki->tx;
   H->nty = (H->n[1] + H->ki->ty - 1) / H->ki->ty;
+  for (int k = 0; k < 2; ++k)
+    if (H->gexec[k]) {
+      cudaGraphExecDestroy(H->gexec[k]);
+      H->gexec[k] = nullptr;
+    }
 
-  int dev = 0;
-  SP_CUDA(H, cudaGetDevice(&dev));
-  SP_CUDA(H, cudaDeviceGetAttribute(&H->sms, cudaDevAttrMultiProcessorCount, dev));
-  SP_CUDA(H, cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking));
-  H->own_stream = true;
-
-  const size_t bytes = size_t(H->batch) * H->nf * H->felems * H->esz;
-  for (int k = 0; k < 2; ++k) {
-    if (cudaMalloc(&H->buf[k], bytes) != cudaSuccess)
-      return fail(H, SP_ENOMEM, "device allocation of the field buffers failed");
-    SP_CUDA(H, cudaMemset(H->buf[k], 0, bytes));
-  }
-
-  // TMA descriptors of every field of both buffers, and output origins
   EncodeTiled enc = encode_fn();
   if (!enc) return fail(H, SP_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
   const int cnt = H->batch * H->nf;
@@ -436,10 +412,10 @@ int create(const sp_desc* desc, sp_handle* H) {
           return fail(H, SP_ECUDA, b);
         }
       }
-    SP_CUDA(H, cudaMalloc(&H->maps_d[k], sizeof(CUtensorMap) * cnt));
+    if (!H->maps_d[k]) SP_CUDA(H, cudaMalloc(&H->maps_d[k], sizeof(CUtensorMap) * cnt));
     SP_CUDA(H, cudaMemcpy(H->maps_d[k], maps.data(), sizeof(CUtensorMap) * cnt,
                           cudaMemcpyHostToDevice));
-    SP_CUDA(H, cudaMalloc(&H->outs_d[k], sizeof(void*) * cnt));
+    if (!H->outs_d[k]) SP_CUDA(H, cudaMalloc(&H->outs_d[k], sizeof(void*) * cnt));
     SP_CUDA(H, cudaMemcpy(H->outs_d[k], outs.data(), sizeof(void*) * cnt, cudaMemcpyHostToDevice));
   }
 
@@ -464,12 +440,92 @@ int create(const sp_desc* desc, sp_handle* H) {
     if (rc) return rc;
     partial_n = std::max(partial_n, size_t(H->grid2));
   }
-  H->partial_n = partial_n;
-  SP_CUDA(H, cudaMalloc(&H->partial_d, sizeof(double) * partial_n));
+  if (partial_n > H->partial_n) {
+    cudaFree(H->partial_d);
+    H->partial_d = nullptr;
+    H->partial_n = partial_n;
+    SP_CUDA(H, cudaMalloc(&H->partial_d, sizeof(double) * partial_n));
+  }
+  return SP_OK;
+}
+
+// fastest tile shape of each (kernel key, extents, batch) found so far
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int>, int> g_tuned;
+
+std::tuple<int, int, int, int, int, int, int, int, int, int, int> tune_key(const sp_handle* H) {
+  const sp_desc& d = H->d;
+  return {d.model, d.form, d.dim, d.dtype, d.lap_pts, d.gradlap_pts, d.bilap_pts,
+          H->n[0], H->n[1], H->n[2], H->batch};
+}
+
+int create(const sp_desc* desc, sp_handle* H) {
+  std::string why;
+  if (int rc = validate(desc, why)) return fail(H, rc, why);
+  sp::register_all_kernels();
+  H->d = *desc;
+  H->dim = desc->dim;
+  H->batch = desc->batch;
+  H->esz = desc->dtype == SP_F32 ? 4 : 8;
+  const sp::KernelKey key{desc->model, desc->form, desc->dim, desc->dtype,
+                          desc->lap_pts, desc->gradlap_pts, desc->bilap_pts};
+  const std::vector<sp::KernelInfo>* vs = sp::find_kernels(key);
+  if (!vs || vs->empty()) {
+    char b[256];
+    snprintf(b, sizeof b,
+             "no fused kernel built for model %d form %d dim %d dtype %d stencil <%d,%d,%d>",
+             desc->model, desc->form, desc->dim, desc->dtype, desc->lap_pts,
+             desc->gradlap_pts, desc->bilap_pts);
+    return fail(H, SP_EINVAL, b);
+  }
+  H->variants = *vs;
+  H->ki = &H->variants[0];
+  H->nf = H->ki->nf;
+  for (int a = 0; a < 3; ++a) H->n[a] = (a < H->dim) ? desc->n[a] : 1;
+  const int R = H->ki->R;
+  for (int a = 0; a < H->dim; ++a)
+    if (H->n[a] < 2 * R) return fail(H, SP_EINVAL, "an extent is smaller than twice the stencil reach");
+  H->h[0] = H->ki->hx;
+  H->h[1] = R;
+  H->h[2] = H->dim == 3 ? R : 0;
+  for (const sp::KernelInfo& v : H->variants)
+    if (v.hx != H->h[0] || v.R != R || v.nf != H->nf)
+      return fail(H, SP_EINVAL, "tile variants of one kernel disagree on the halo");
+  const int va = int(16 / H->esz);
+  H->pitch = ((H->n[0] + 2 * H->h[0] + va - 1) / va) * va;
+  H->ly = H->n[1] + 2 * H->h[1];
+  H->lz = H->dim == 3 ? H->n[2] + 2 * H->h[2] : 1;
+  H->plane = H->pitch * H->ly;
+  H->felems = ((H->plane * H->lz + 63) / 64) * 64;
+
+  int dev = 0;
+  SP_CUDA(H, cudaGetDevice(&dev));
+  SP_CUDA(H, cudaDeviceGetAttribute(&H->sms, cudaDevAttrMultiProcessorCount, dev));
+  SP_CUDA(H, cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking));
+  H->own_stream = true;
+
+  const size_t bytes = size_t(H->batch) * H->nf * H->felems * H->esz;
+  for (int k = 0; k < 2; ++k) {
+    if (cudaMalloc(&H->buf[k], bytes) != cudaSuccess)
+      return fail(H, SP_ENOMEM, "device allocation of the field buffers failed");
+    SP_CUDA(H, cudaMemset(H->buf[k], 0, bytes));
+  }
   SP_CUDA(H, cudaMalloc(&H->result_d, sizeof(double) * (2 + H->batch)));
   SP_CUDA(H, cudaMallocHost(&H->result_h, sizeof(double) * (2 + H->batch)));
   SP_CUDA(H, cudaMalloc(&H->err_d, sizeof(int)));
   SP_CUDA(H, cudaMemset(H->err_d, 0, sizeof(int)));
+
+  // tile shape: an explicit choice (SP_TILE), else the one sp_autotune found
+  // for this kernel and size in this process, else the first registered
+  int variant = 0;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    auto it = g_tuned.find(tune_key(H));
+    if (it != g_tuned.end()) variant = it->second;
+  }
+  if (const char* t = getenv("SP_TILE")) variant = atoi(t);
+  if (variant < 0 || variant >= int(H->variants.size())) variant = 0;
+  if (int rc = configure(H, variant)) return rc;
   SP_CUDA(H, cudaDeviceSynchronize());
   return SP_OK;
 }
@@ -696,6 +752,59 @@ int sp_reduce(sp_handle* H, int inst, int field, double* mass, double* energy) {
     return fail(H, SP_EINVAL, "instance or field index out of range");
   return H->esz == 4 ? reduce_t<float>(H, inst, field, mass, energy)
                      : reduce_t<double>(H, inst, field, mass, energy);
+}
+
+int sp_autotune(sp_handle* H, int reps) {
+  if (!H || reps < 1) return SP_EINVAL;
+  if (H->variants.size() < 2) return SP_OK;
+  const long long launches = H->launches;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  SP_CUDA(H, cudaEventCreate(&e0));
+  SP_CUDA(H, cudaEventCreate(&e1));
+  int best = H->variant;
+  float best_ms = 1e30f;
+  int rc = SP_OK;
+  for (int v = 0; v < int(H->variants.size()) && rc == SP_OK; ++v) {
+    if ((rc = configure(H, v))) break;
+    // right-hand-side launches: the same loads and stores as a step, and the
+    // state of the model is left untouched
+    for (int i = 0; i < 2 && rc == SP_OK; ++i) rc = launch_step(H, 1, nullptr);
+    cudaEventRecord(e0, H->stream);
+    for (int i = 0; i < reps && rc == SP_OK; ++i) rc = launch_step(H, 1, nullptr);
+    cudaEventRecord(e1, H->stream);
+    if (rc) break;
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      rc = fail(H, SP_ECUDA, "autotune timing failed");
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  H->launches = launches;
+  if (rc) return rc;
+  if ((rc = configure(H, best))) return rc;
+  std::lock_guard<std::mutex> lk(g_tune_mutex);
+  g_tuned[tune_key(H)] = best;
+  return check_err_flag(H);
+}
+
+int sp_kernel_info(const sp_handle* H, int info[8]) {
+  if (!H || !info) return SP_EINVAL;
+  info[0] = H->ki->tx;
+  info[1] = H->ki->ty;
+  info[2] = H->ki->spt;
+  info[3] = H->ki->pd;
+  info[4] = H->variant;
+  info[5] = int(H->variants.size());
+  info[6] = H->ki->threads;
+  info[7] = H->dim == 3 ? H->zchunk : H->grid2;
+  return SP_OK;
 }
 
 int sp_set_dt(sp_handle* H, double dt) {

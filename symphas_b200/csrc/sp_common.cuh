@@ -53,6 +53,55 @@ __device__ __forceinline__ Vec<T, W> operator-(const Vec<T, W>& a) {
   return r;
 }
 
+// Two FP32 lanes map onto Blackwell's packed FP32x2 instructions
+// (add/sub/mul/fma .rn.f32x2, sm_100a): one instruction per two sites, each
+// lane rounded exactly as the scalar operation.
+#define SP_F32X2_OP(NAME, OPC)                                                          \
+  __device__ __forceinline__ Vec<float, 2> NAME(const Vec<float, 2>& a, const Vec<float, 2>& b) { \
+    Vec<float, 2> r;                                                                    \
+    asm("{.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t" OPC      \
+        " d, a, b;\n\tmov.b64 {%0, %1}, d;}"                                             \
+        : "=f"(r.v[0]), "=f"(r.v[1])                                                    \
+        : "f"(a.v[0]), "f"(a.v[1]), "f"(b.v[0]), "f"(b.v[1]));                          \
+    return r;                                                                           \
+  }
+SP_F32X2_OP(operator+, "add.rn.f32x2")
+SP_F32X2_OP(operator-, "sub.rn.f32x2")
+SP_F32X2_OP(operator*, "mul.rn.f32x2")
+#undef SP_F32X2_OP
+
+__device__ __forceinline__ Vec<float, 2> fma_op(const Vec<float, 2>& a, const Vec<float, 2>& b,
+                                                 const Vec<float, 2>& c) {
+  Vec<float, 2> r;
+  asm("{.reg .b64 a, b, c, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
+      "mov.b64 c, {%6, %7};\n\tfma.rn.f32x2 d, a, b, c;\n\tmov.b64 {%0, %1}, d;}"
+      : "=f"(r.v[0]), "=f"(r.v[1])
+      : "f"(a.v[0]), "f"(a.v[1]), "f"(b.v[0]), "f"(b.v[1]), "f"(c.v[0]), "f"(c.v[1]));
+  return r;
+}
+__device__ __forceinline__ float fma_op(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_op(double a, double b, double c) { return __fma_rn(a, b, c); }
+template <class T, int W>
+__device__ __forceinline__ Vec<T, W> fma_op(const Vec<T, W>& a, const Vec<T, W>& b,
+                                            const Vec<T, W>& c) {
+  Vec<T, W> r;
+#pragma unroll
+  for (int j = 0; j < W; ++j) r.v[j] = fma_op(a.v[j], b.v[j], c.v[j]);
+  return r;
+}
+
+// a * b + c: one rounding (FMA) when CONTRACT, else a rounded product and then
+// a rounded sum, as the exact form requires
+template <bool CONTRACT, class V>
+__device__ __forceinline__ V fmadd(const V& a, const V& b, const V& c) {
+  if constexpr (CONTRACT) {
+    return fma_op(a, b, c);
+  } else {
+    const V p = a * b;
+    return p + c;
+  }
+}
+
 template <class T, int W>
 struct VecOf {
   using type = Vec<T, W>;
@@ -106,11 +155,12 @@ __device__ __forceinline__ vec_t<T, W> load_at(const T* p) {
 // Evaluation context of one W-wide site group: shared-memory offsets of the
 // field planes (NZ planes centred at ZR) and staged-operand planes, relative
 // to `base`; PW and SW are the row pitches of the field and stage tiles.
-template <class T, int W, int DIM, int LP, int GP, int BP, int NF, int NZ, int ZR, int PW,
-          int NS, int NSZ, int SZR, int SW>
+template <class T, int W, bool CONTRACT, int DIM, int LP, int GP, int BP, int NF, int NZ, int ZR,
+          int PW, int NS, int NSZ, int SZR, int SW>
 struct Ctx {
   using scalar_type = T;
   using value_type = vec_t<T, W>;
+  static constexpr bool contract = CONTRACT;  // a*b + c may round once
   static constexpr int dim = DIM, lap_points = LP, gradlap_points = GP, bilap_points = BP;
   const T* base;
   int fo[NF][NZ];

@@ -26,6 +26,7 @@
 
 #include <type_traits>
 
+#include "sp_common.cuh"
 #include "sp_stencils.cuh"
 
 #ifndef __CUDACC__
@@ -267,6 +268,70 @@ struct Ev<Mul<A, B>> {
     return Ev<A>::template at<X, Y, Z>(e.a, c) * Ev<B>::template at<X, Y, Z>(e.b, c);
   }
 };
+// a*b + c and its relatives: one FMA when the context may contract; in the
+// exact form the same rounded product and rounded sum as the plain nodes
+// (c + p = p + c and c - p = (-a)*b + c bit for bit)
+template <class A, class B, class C2>
+struct Ev<Add<Mul<A, B>, C2>> {
+  template <int X, int Y, int Z, class C>
+  __device__ __forceinline__ static typename C::value_type at(const Add<Mul<A, B>, C2>& e,
+                                                              const C& c) {
+    return fmadd<C::contract>(Ev<A>::template at<X, Y, Z>(e.a.a, c),
+                              Ev<B>::template at<X, Y, Z>(e.a.b, c),
+                              Ev<C2>::template at<X, Y, Z>(e.b, c));
+  }
+};
+template <class C2, class A, class B>
+struct Ev<Add<C2, Mul<A, B>>> {
+  template <int X, int Y, int Z, class C>
+  __device__ __forceinline__ static typename C::value_type at(const Add<C2, Mul<A, B>>& e,
+                                                              const C& c) {
+    return fmadd<C::contract>(Ev<A>::template at<X, Y, Z>(e.b.a, c),
+                              Ev<B>::template at<X, Y, Z>(e.b.b, c),
+                              Ev<C2>::template at<X, Y, Z>(e.a, c));
+  }
+};
+template <class A, class B, class A2, class B2>
+struct Ev<Add<Mul<A, B>, Mul<A2, B2>>> {  // left product first, as written
+  template <int X, int Y, int Z, class C>
+  __device__ __forceinline__ static typename C::value_type at(
+      const Add<Mul<A, B>, Mul<A2, B2>>& e, const C& c) {
+    return fmadd<C::contract>(Ev<A2>::template at<X, Y, Z>(e.b.a, c),
+                              Ev<B2>::template at<X, Y, Z>(e.b.b, c),
+                              Ev<Mul<A, B>>::template at<X, Y, Z>(e.a, c));
+  }
+};
+template <class C2, class A, class B>
+struct Ev<Sub<C2, Mul<A, B>>> {
+  template <int X, int Y, int Z, class C>
+  __device__ __forceinline__ static typename C::value_type at(const Sub<C2, Mul<A, B>>& e,
+                                                              const C& c) {
+    return fmadd<C::contract>(-Ev<A>::template at<X, Y, Z>(e.b.a, c),
+                              Ev<B>::template at<X, Y, Z>(e.b.b, c),
+                              Ev<C2>::template at<X, Y, Z>(e.a, c));
+  }
+};
+template <class A, class B, class C2>
+struct Ev<Sub<Mul<A, B>, C2>> {
+  template <int X, int Y, int Z, class C>
+  __device__ __forceinline__ static typename C::value_type at(const Sub<Mul<A, B>, C2>& e,
+                                                              const C& c) {
+    return fmadd<C::contract>(Ev<A>::template at<X, Y, Z>(e.a.a, c),
+                              Ev<B>::template at<X, Y, Z>(e.a.b, c),
+                              -Ev<C2>::template at<X, Y, Z>(e.b, c));
+  }
+};
+template <class A, class B, class A2, class B2>
+struct Ev<Sub<Mul<A, B>, Mul<A2, B2>>> {
+  template <int X, int Y, int Z, class C>
+  __device__ __forceinline__ static typename C::value_type at(
+      const Sub<Mul<A, B>, Mul<A2, B2>>& e, const C& c) {
+    return fmadd<C::contract>(-Ev<A2>::template at<X, Y, Z>(e.b.a, c),
+                              Ev<B2>::template at<X, Y, Z>(e.b.b, c),
+                              Ev<Mul<A, B>>::template at<X, Y, Z>(e.a, c));
+  }
+};
+
 template <class A>
 struct Ev<Neg<A>> {
   template <int X, int Y, int Z, class C>

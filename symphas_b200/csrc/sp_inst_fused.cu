@@ -25,9 +25,24 @@
   SP_REG3(SPK_B, SPK_FUSED, MF_B_exact, T, DT, 15, 10, 25);                          \
   SP_REG3(SPK_C, SPK_FUSED, MF_C_exact, T, DT, 15, 10, 25);
 
+// extra tile shapes of the FP32 fused kernels, for sp_autotune
+#define SP_FUSED_VARIANTS3(MODEL, MF)                                                   \
+  SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3b);        \
+  SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3c);        \
+  SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3d);
+#define SP_FUSED_VARIANTS2(MODEL, MF0, MF1)                                             \
+  SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2b);   \
+  SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2c);
+
 namespace sp {
 void register_fused_kernels() {
   SP_FUSED_SET(float, 0)
   SP_FUSED_SET(double, 1)
+  SP_FUSED_VARIANTS3(SPK_A, MF_A_fused)
+  SP_FUSED_VARIANTS3(SPK_B, MF_B_fused)
+  SP_FUSED_VARIANTS3(SPK_C, MF_C_fused)
+  SP_FUSED_VARIANTS2(SPK_A, MF_A_fused, MF_A_fused)
+  SP_FUSED_VARIANTS2(SPK_B, MF_B_fused, MF_B_fused)
+  SP_FUSED_VARIANTS2(SPK_ENS_AB, MF_AMK_fused, MF_BMK_fused)
 }
 }  // namespace sp

@@ -112,15 +112,32 @@ template <class T, int W, int DIM, int R>
 __device__ __forceinline__ void store_group(T* org, int x, int y, int z, const vec_t<T, W>& v,
                                             const int* n, const int* h, const int* per,
                                             long long pitch, long long plane) {
-  const bool edge = (per[0] && (x < R || x + W > n[0] - R)) ||
-                    (per[1] && (y < R || y >= n[1] - R)) ||
-                    (DIM == 3 && per[2] && (z < R || z >= n[2] - R));
-  T* p = org + ((DIM == 3) ? (long long)(z + h[2]) * plane : 0) + (long long)(y + h[1]) * pitch +
-         (x + h[0]);
-  if (!edge && x + W <= n[0]) {
-    *reinterpret_cast<vec_t<T, W>*>(p) = v;
+  if (x + W <= n[0] && n[0] % W == 0) {
+    // whole group: it and each of its periodic images is one vector store
+    int xs[2] = {x + h[0], 0}, ys[2] = {y + h[1], 0}, zs[2] = {DIM == 3 ? z + h[2] : 0, 0};
+    int cx = 1, cy = 1, cz = 1;
+    if (R > 0) {
+      if (per[0]) {
+        if (x < R) xs[cx++] = xs[0] + n[0];
+        else if (x + W > n[0] - R) xs[cx++] = xs[0] - n[0];
+      }
+      if (per[1]) {
+        if (y < R) ys[cy++] = ys[0] + n[1];
+        else if (y >= n[1] - R) ys[cy++] = ys[0] - n[1];
+      }
+      if (DIM == 3 && per[2]) {
+        if (z < R) zs[cz++] = zs[0] + n[2];
+        else if (z >= n[2] - R) zs[cz++] = zs[0] - n[2];
+      }
+    }
+    for (int k = 0; k < cz; ++k)
+      for (int j = 0; j < cy; ++j)
+        for (int i = 0; i < cx; ++i)
+          *reinterpret_cast<vec_t<T, W>*>(org + (long long)zs[k] * plane +
+                                          (long long)ys[j] * pitch + xs[i]) = v;
     return;
   }
+  // ragged end of a row: element by element
 #pragma unroll
   for (int j = 0; j < W; ++j) {
     const int xj = x + j;
@@ -149,6 +166,15 @@ __device__ __forceinline__ void store_group(T* org, int x, int y, int z, const v
   }
 }
 
+// (s + d) mod N for 0 <= s < N and |d| < N, without a division
+template <int N>
+__device__ __forceinline__ int wrap(int s, int d) {
+  int r = s + d;
+  r += (r < 0) ? N : 0;
+  r -= (r >= N) ? N : 0;
+  return r;
+}
+
 template <class T, int W>
 __device__ __forceinline__ double vsum(const vec_t<T, W>& v, int x, int n0) {
   double s = 0.0;
@@ -166,7 +192,7 @@ __device__ __forceinline__ double vsum(const vec_t<T, W>& v, int x, int n0) {
 // of plane zi.  The field planes it needs lie in the window [zi + L, zi + U],
 // so the shared-memory ring holds U - L + 1 planes plus PD in flight.
 // ---------------------------------------------------------------------------
-template <class M, class T, int LP, int GP, int BP, class TC>
+template <class M, class T, int LP, int GP, int BP, class TC, bool EXACT>
 struct Fd3 {
   static constexpr int TX = TC::TX, TY = TC::TY, SPT = TC::SPT, PD = TC::PD, W = TC::W,
                        TXT = TC::TXT, NT = TC::NT;
@@ -198,10 +224,10 @@ struct Fd3 {
   static_assert(NE <= NT, "one extra stage cell per thread at most");
 };
 
-template <class M, class T, int LP, int GP, int BP, class TC>
+template <class M, class T, int LP, int GP, int BP, class TC, bool EXACT>
 __global__ void __launch_bounds__(TC::NT)
     k_fd3d(const __grid_constant__ StepParams<T> p, const __grid_constant__ M m) {
-  using K = Fd3<M, T, LP, GP, BP, TC>;
+  using K = Fd3<M, T, LP, GP, BP, TC, EXACT>;
   constexpr int TX = K::TX, TY = K::TY, SPT = K::SPT, PD = K::PD, W = K::W, TXT = K::TXT,
                 NF = K::NF, NS = K::NS, R = K::R, RS = K::RS, RSA = K::RSA, HXA = K::HXA,
                 PW = K::PW, PH = K::PH, PLANE = K::PLANE, NSLOT = K::NSLOT, SW = K::SW,
@@ -285,8 +311,13 @@ __global__ void __launch_bounds__(TC::NT)
 
   double msum = 0.0;
   int waited = -1;
+  // ring slot of plane zi (field ring) and of staged plane zi (stage ring),
+  // advanced by one per iteration instead of divided out
+  int zslot = ((zi0 - (zb - R)) % NSLOT + NSLOT) % NSLOT;
+  int sslot0 = NS > 0 ? ((zi0 - (zb - RS)) % (NSR > 0 ? NSR : 1) + NSR) % (NSR > 0 ? NSR : 1) : 0;
 
-  for (int zi = zi0; zi < ze; ++zi) {
+  for (int zi = zi0; zi < ze; ++zi, zslot = wrap<NSLOT>(zslot, 1),
+           sslot0 = NS > 0 ? wrap<(NSR > 0 ? NSR : 1)>(sslot0, 1) : 0) {
     const int qn = zi + U + PD - (zb - R);
     if (tid == 0 && qn < nplanes) issue(qn);
     bool bad = false;
@@ -295,17 +326,15 @@ __global__ void __launch_bounds__(TC::NT)
     waited = qw;
 
     if constexpr (NS > 0) {
-      using CS = Ctx<T, W, 3, LP, GP, BP, NF, 2 * RI + 1, RI, PW, 1, 1, 0, SW>;
-      const int zs = zi + RS;
-      const int qs = zs - (zb - R);
-      T* sdst = sbuf + ((zs - (zb - RS)) % NSR) * SPL;
+      using CS = Ctx<T, W, !EXACT, 3, LP, GP, BP, NF, 2 * RI + 1, RI, PW, 1, 1, 0, SW>;
+      T* sdst = sbuf + wrap<NSR>(sslot0, RS) * SPL;
       CS c0;
       c0.base = fbuf;
 #pragma unroll
       for (int f = 0; f < NF; ++f)
 #pragma unroll
         for (int dz = -RI; dz <= RI; ++dz)
-          c0.fo[f][dz + RI] = (f * NSLOT + (qs + dz) % NSLOT) * PLANE;
+          c0.fo[f][dz + RI] = (f * NSLOT + wrap<NSLOT>(zslot, RS + dz)) * PLANE;
       c0.divh2 = vdivh2;
       c0.divh3 = vdivh3;
       c0.divh4 = vdivh4;
@@ -344,9 +373,8 @@ __global__ void __launch_bounds__(TC::NT)
 
     if (zi >= zb) {
       const int z = zi;
-      const int qz = z - (zb - R);
-      using CO = Ctx<T, W, 3, LP, GP, BP, NF, 2 * RD + 1, RD, PW, NS, (NS > 0 ? 2 * RS + 1 : 1),
-                     (NS > 0 ? RS : 0), SW>;
+      using CO = Ctx<T, W, !EXACT, 3, LP, GP, BP, NF, 2 * RD + 1, RD, PW, NS,
+                     (NS > 0 ? 2 * RS + 1 : 1), (NS > 0 ? RS : 0), SW>;
       CO c0;
       c0.base = fbuf;
       const int cell = (row0 + R) * PW + txt * W + HXA;
@@ -354,14 +382,14 @@ __global__ void __launch_bounds__(TC::NT)
       for (int f = 0; f < NF; ++f)
 #pragma unroll
         for (int dz = -RD; dz <= RD; ++dz)
-          c0.fo[f][dz + RD] = (f * NSLOT + (qz + dz) % NSLOT) * PLANE + cell;
+          c0.fo[f][dz + RD] = (f * NSLOT + wrap<NSLOT>(zslot, dz)) * PLANE + cell;
       if constexpr (NS > 0) {
         const int scell = int(sbuf - fbuf) + (row0 + RS) * SW + txt * W + RSA;
 #pragma unroll
         for (int k = 0; k < NS; ++k)
 #pragma unroll
           for (int dz = -RS; dz <= RS; ++dz)
-            c0.so[k][dz + RS] = (k * NSR + (z + dz - (zb - RS)) % NSR) * SPL + scell;
+            c0.so[k][dz + RS] = (k * NSR + wrap<NSR>(sslot0, dz)) * SPL + scell;
       }
       c0.divh2 = vdivh2;
       c0.divh3 = vdivh3;
@@ -382,10 +410,10 @@ __global__ void __launch_bounds__(TC::NT)
             for (int dz = 0; dz < 2 * RS + 1; ++dz) ctx.so[kk][dz] += k * SW;
         }
         const V r0 = eval(m.r0, ctx);
-        nv[k][0] = p.rhs_only ? r0 : ctx.template var<1, 0, 0, 0>() + vdt * r0;
+        nv[k][0] = p.rhs_only ? r0 : fmadd<!EXACT>(vdt, r0, ctx.template var<1, 0, 0, 0>());
         if constexpr (NF > 1) {
           const V r1 = eval(m.r1, ctx);
-          nv[k][1] = p.rhs_only ? r1 : ctx.template var<2, 0, 0, 0>() + vdt * r1;
+          nv[k][1] = p.rhs_only ? r1 : fmadd<!EXACT>(vdt, r1, ctx.template var<2, 0, 0, 0>());
         }
       }
       const long long zoff = (long long)(z + p.h[2]) * p.plane;
@@ -420,8 +448,9 @@ __global__ void __launch_bounds__(TC::NT)
 // One barrier per tile: the tile ring keeps PD tiles in flight plus two being
 // read, and the stage buffer alternates between two copies.
 // ---------------------------------------------------------------------------
-template <class M0, class M1, class T, int LP, int GP, int BP, class TC>
+template <class M0, class M1, class T, int LP, int GP, int BP, class TC, bool EXACT>
 struct Fd2 {
+  static constexpr bool exact = EXACT;
   static_assert(M0::nf == M1::nf, "models of one launch share the field count");
   static constexpr int TX = TC::TX, TY = TC::TY, SPT = TC::SPT, PD = TC::PD, W = TC::W,
                        TXT = TC::TXT, NT = TC::NT;
@@ -457,7 +486,7 @@ __device__ __forceinline__ void fd2_stage(const M& m, const Inst2<T>& ip, const 
   constexpr int NS = M::ns;
   constexpr int SO = NS > 1 ? 2 : 1;
   using V = vec_t<T, W>;
-  using CS = Ctx<T, W, 2, LP, GP, BP, NF, 1, 0, PW, 1, 1, 0, SW>;
+  using CS = Ctx<T, W, !K::exact, 2, LP, GP, BP, NF, 1, 0, PW, 1, 1, 0, SW>;
   const int tid = threadIdx.x, txt = tid % TXT, row0 = (tid / TXT) * SPT;
   T coef[8];
 #pragma unroll
@@ -506,7 +535,7 @@ __device__ __forceinline__ void fd2_out(const Step2Params<T>& p, const M& m, con
   for (int i = 0; i < 8; ++i) coef[i] = ip.coef[i];
   const int n0 = ip.n[0], n1 = ip.n[1];
   const long long pitch = ip.pitch;
-  using CO = Ctx<T, W, 2, LP, GP, BP, NF, 1, 0, PW, NS, 1, 0, SW>;
+  using CO = Ctx<T, W, !K::exact, 2, LP, GP, BP, NF, 1, 0, PW, NS, 1, 0, SW>;
   CO c0;
   c0.base = fbuf;
   const int cell = (row0 + R) * PW + txt * W + HXA;
@@ -534,10 +563,10 @@ __device__ __forceinline__ void fd2_out(const Step2Params<T>& p, const M& m, con
       for (int kk = 0; kk < NS; ++kk) ctx.so[kk][0] += k * SW;
     }
     const V r0 = eval(m.r0, ctx);
-    nv[k][0] = p.rhs_only ? r0 : ctx.template var<1, 0, 0, 0>() + vdt * r0;
+    nv[k][0] = p.rhs_only ? r0 : fmadd<!K::exact>(vdt, r0, ctx.template var<1, 0, 0, 0>());
     if constexpr (NF > 1) {
       const V r1 = eval(m.r1, ctx);
-      nv[k][1] = p.rhs_only ? r1 : ctx.template var<2, 0, 0, 0>() + vdt * r1;
+      nv[k][1] = p.rhs_only ? r1 : fmadd<!K::exact>(vdt, r1, ctx.template var<2, 0, 0, 0>());
     }
   }
   const bool xedge = (ip.per[0] && (x < R || x + W > n0 - R)) || (x + W > n0);
@@ -562,11 +591,11 @@ __device__ __forceinline__ void fd2_out(const Step2Params<T>& p, const M& m, con
   }
 }
 
-template <class M0, class M1, class T, int LP, int GP, int BP, class TC>
+template <class M0, class M1, class T, int LP, int GP, int BP, class TC, bool EXACT>
 __global__ void __launch_bounds__(TC::NT)
     k_fd2d(const __grid_constant__ Step2Params<T> p, const __grid_constant__ M0 m0,
            const __grid_constant__ M1 m1) {
-  using K = Fd2<M0, M1, T, LP, GP, BP, TC>;
+  using K = Fd2<M0, M1, T, LP, GP, BP, TC, EXACT>;
   constexpr int TX = K::TX, TY = K::TY, PD = K::PD, NQ = K::NQ, NF = K::NF, R = K::R,
                 HXA = K::HXA, PW = K::PW, PH = K::PH, PLANE = K::PLANE, NT = K::NT,
                 NS = K::NS, RS = K::RS, SWC = K::SWC, XC = K::XC, NE = K::NE, TXT = K::TXT;

@@ -12,12 +12,12 @@ namespace sp {
 template <class MF>
 using model_of = decltype(MF{}());
 
-template <class MF, class T, int LP, int GP, int BP, class TC>
+template <class MF, class T, int LP, int GP, int BP, class TC, bool EXACT>
 struct Entry3 {
   using M = model_of<MF>;
-  using K = Fd3<M, T, LP, GP, BP, TC>;
+  using K = Fd3<M, T, LP, GP, BP, TC, EXACT>;
   static cudaError_t launch(const void* prm, dim3 grid, cudaStream_t s) {
-    auto kern = k_fd3d<M, T, LP, GP, BP, TC>;
+    auto kern = k_fd3d<M, T, LP, GP, BP, TC, EXACT>;
     static cudaError_t attr = cudaFuncSetAttribute(
         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
     if (attr != cudaSuccess) return attr;
@@ -26,7 +26,7 @@ struct Entry3 {
     return cudaGetLastError();
   }
   static int occupancy() {
-    auto kern = k_fd3d<M, T, LP, GP, BP, TC>;
+    auto kern = k_fd3d<M, T, LP, GP, BP, TC, EXACT>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, K::NT, K::SMEM) != cudaSuccess)
@@ -34,17 +34,18 @@ struct Entry3 {
     return n > 0 ? n : 1;
   }
   static KernelInfo info() {
-    return KernelInfo{K::NF, K::NS, K::R, K::HXA, K::TX, K::TY, K::NT, K::SMEM, &launch, &occupancy};
+    return KernelInfo{K::NF, K::NS,     K::R,    K::HXA,  K::TX,      K::TY,
+                      K::SPT, K::PD, K::NT, K::SMEM, &launch, &occupancy};
   }
 };
 
-template <class MF0, class MF1, class T, int LP, int GP, int BP, class TC>
+template <class MF0, class MF1, class T, int LP, int GP, int BP, class TC, bool EXACT>
 struct Entry2 {
   using M0 = model_of<MF0>;
   using M1 = model_of<MF1>;
-  using K = Fd2<M0, M1, T, LP, GP, BP, TC>;
+  using K = Fd2<M0, M1, T, LP, GP, BP, TC, EXACT>;
   static cudaError_t launch(const void* prm, dim3 grid, cudaStream_t s) {
-    auto kern = k_fd2d<M0, M1, T, LP, GP, BP, TC>;
+    auto kern = k_fd2d<M0, M1, T, LP, GP, BP, TC, EXACT>;
     static cudaError_t attr = cudaFuncSetAttribute(
         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
     if (attr != cudaSuccess) return attr;
@@ -54,7 +55,7 @@ struct Entry2 {
     return cudaGetLastError();
   }
   static int occupancy() {
-    auto kern = k_fd2d<M0, M1, T, LP, GP, BP, TC>;
+    auto kern = k_fd2d<M0, M1, T, LP, GP, BP, TC, EXACT>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, K::NT, K::SMEM) != cudaSuccess)
@@ -62,7 +63,8 @@ struct Entry2 {
     return n > 0 ? n : 1;
   }
   static KernelInfo info() {
-    return KernelInfo{K::NF, K::NS, K::R, K::HXA, K::TX, K::TY, K::NT, K::SMEM, &launch, &occupancy};
+    return KernelInfo{K::NF, K::NS,     K::R,    K::HXA,  K::TX,      K::TY,
+                      K::SPT, K::PD, K::NT, K::SMEM, &launch, &occupancy};
   }
 };
 
@@ -109,6 +111,12 @@ template <class T> struct Tiles;
 template <> struct Tiles<float> {
   using D3 = TileCfg<64, 16, 2, 4, 2>;
   using D2 = TileCfg<128, 16, 4, 3, 2>;
+  // further shapes the autotuner tries for the headline (fused FP32) kernels
+  using D3b = TileCfg<64, 32, 4, 2, 2>;
+  using D3c = TileCfg<64, 16, 4, 4, 2>;
+  using D3d = TileCfg<128, 16, 4, 2, 2>;
+  using D2b = TileCfg<64, 32, 4, 3, 2>;
+  using D2c = TileCfg<128, 32, 8, 2, 2>;
 };
 template <> struct Tiles<double> {
   using D3 = TileCfg<64, 16, 2, 3, 2>;
@@ -118,10 +126,16 @@ template <> struct Tiles<double> {
 
 #define SP_REG3(MODEL, FORM, MF, T, DT, LP, GP, BP)                        \
   ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 3, DT, LP, GP, BP},    \
-                        ::sp::Entry3<::sp::MF, T, LP, GP, BP, ::sp::Tiles<T>::D3>::info())
+                        ::sp::Entry3<::sp::MF, T, LP, GP, BP, ::sp::Tiles<T>::D3, FORM == SPK_EXACT>::info())
 #define SP_REG2(MODEL, FORM, MF, T, DT, LP, GP, BP)                        \
   ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 2, DT, LP, GP, BP},    \
-                        ::sp::Entry2<::sp::MF, ::sp::MF, T, LP, GP, BP, ::sp::Tiles<T>::D2>::info())
+                        ::sp::Entry2<::sp::MF, ::sp::MF, T, LP, GP, BP, ::sp::Tiles<T>::D2, FORM == SPK_EXACT>::info())
+#define SP_REG3T(MODEL, FORM, MF, T, DT, LP, GP, BP, TILE)                  \
+  ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 3, DT, LP, GP, BP},    \
+                        ::sp::Entry3<::sp::MF, T, LP, GP, BP, TILE, FORM == SPK_EXACT>::info())
+#define SP_REG2T(MODEL, FORM, MF0, MF1, T, DT, LP, GP, BP, TILE)            \
+  ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 2, DT, LP, GP, BP},    \
+                        ::sp::Entry2<::sp::MF0, ::sp::MF1, T, LP, GP, BP, TILE, FORM == SPK_EXACT>::info())
 #define SP_REG2X(MODEL, FORM, MF0, MF1, T, DT, LP, GP, BP)                 \
   ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 2, DT, LP, GP, BP},    \
-                        ::sp::Entry2<::sp::MF0, ::sp::MF1, T, LP, GP, BP, ::sp::Tiles<T>::D2>::info())
+                        ::sp::Entry2<::sp::MF0, ::sp::MF1, T, LP, GP, BP, ::sp::Tiles<T>::D2, FORM == SPK_EXACT>::info())

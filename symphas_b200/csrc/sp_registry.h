@@ -2,14 +2,18 @@
  * sp_registry.h -- table of the fused-step kernels built into the library.
  *
  * Each entry is one (model, form, dimension, dtype, stencil point set) lowered
- * at build time into a kernel instantiation; sp_create looks its description
- * up here, the way SymPhas resolves model_X_t<D, SolverFT<Stencil..>> at
- * compile time (sol/inc/modelmacros.h:597-626, examples/solvers/solverft.h:219-239).
+ * at build time into one or more kernel instantiations that differ only in
+ * their tile shape; sp_create looks the description up here, the way SymPhas
+ * resolves model_X_t<D, SolverFT<Stencil..>> at compile time
+ * (sol/inc/modelmacros.h:597-626, examples/solvers/solverft.h:219-239), and
+ * sp_autotune picks the fastest tile shape on the current GPU.
  */
 #pragma once
 
 #include <cuda_runtime.h>
 #include <stddef.h>
+
+#include <vector>
 
 namespace sp {
 
@@ -21,19 +25,21 @@ struct KernelInfo {
   int nf;       // fields
   int ns;       // staged operands
   int R;        // halo in y and z (stencil reach of the lowered model)
-  int hx;       // halo in x (R rounded up to 16 bytes)
+  int hx;       // halo in x (R rounded up to 16 bytes, or the stage ring)
   int tx, ty;   // tile
+  int spt, pd;  // rows per thread, TMA stages in flight
   int threads;  // threads per CTA
   size_t smem;  // dynamic shared memory per CTA
   // launches one fused step; `params` is StepParams<T> (3D) or Step2Params<T>
   // (2D); `grid` is ignored for 2D (persistent grid from `ctas`)
   cudaError_t (*launch)(const void* params, dim3 grid, cudaStream_t s);
-  // CTAs of this kernel resident per SM (for sizing persistent grids)
+  // CTAs of this kernel resident per SM (for sizing grids)
   int (*occupancy)();
 };
 
+// appends a tile variant for `key` (the first registered is the default)
 void register_kernel(const KernelKey& key, const KernelInfo& info);
-const KernelInfo* find_kernel(const KernelKey& key);
+const std::vector<KernelInfo>* find_kernels(const KernelKey& key);
 void register_all_kernels();
 
 }  // namespace sp

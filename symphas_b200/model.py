@@ -212,6 +212,18 @@ class Model:
                 self._h)
         return m.value, e.value
 
+    def autotune(self, reps=20):
+        """Pick the fastest tile shape for this kernel and size on this GPU."""
+        C.check(C.lib().sp_autotune(self._h, int(reps)), self._h)
+        return self.kernel_info()
+
+    def kernel_info(self):
+        v = (ctypes.c_int * 8)()
+        C.check(C.lib().sp_kernel_info(self._h, v), self._h)
+        keys = ("tile_x", "tile_y", "rows_per_thread", "stages_in_flight", "variant",
+                "variants", "threads", "z_per_cta_or_ctas")
+        return dict(zip(keys, v[:]))
+
     def synchronize(self):
         C.check(C.lib().sp_synchronize(self._h), self._h)
 

@@ -220,3 +220,33 @@ def test_f32_mass_drift_with_fp64_reduction():
     m.step(dt, 1000)
     m1, _ = m.reduce(0)
     assert abs(m1 - m0) <= 1e-4 * abs(m0)
+
+
+@pytest.mark.parametrize("dim,n,cls", [(3, 40, sp.model_MB_t), (3, 24, sp.model_MC_t),
+                                       (2, 200, sp.model_MB_t), (2, 136, sp.model_MA_t)])
+def test_every_tile_shape_gives_the_same_fields(dim, n, cls, monkeypatch):
+    """The autotuner may pick any tile shape: each must give the same bits."""
+    st = S2 if dim == 2 else S3
+    dims = (n,) * dim
+    coeff = (0.5,) if cls is sp.model_MC_t else ()
+    base = cls(dim, sp.SolverFT(st, form="fused"), sp.ProblemParameters(dims, h=1.0),
+               coeff=coeff, dtype="f32")
+    nv = base.kernel_info()["variants"]
+    ref = None
+    for v in range(nv):
+        monkeypatch.setenv("SP_TILE", str(v))
+        m = cls(dim, sp.SolverFT(st, form="fused"), sp.ProblemParameters(dims, h=1.0),
+                coeff=coeff, dtype="f32")
+        assert m.kernel_info()["variant"] == v
+        for f in range(cls.nfields):
+            m.fill_uniform(f, 60 + f, -0.3, 0.1)
+        m.step(0.004, 25)
+        out = np.stack([m.get_field(f) for f in range(cls.nfields)])
+        if ref is None:
+            ref = out
+        else:
+            assert np.array_equal(out, ref), v
+        m.close()
+    monkeypatch.delenv("SP_TILE")
+    base.autotune(3)
+    assert 0 <= base.kernel_info()["variant"] < nv
