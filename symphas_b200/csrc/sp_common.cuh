@@ -54,30 +54,28 @@ __device__ __forceinline__ Vec<T, W> operator-(const Vec<T, W>& a) {
 }
 
 // Two FP32 lanes map onto Blackwell's packed FP32x2 instructions
-// (add/sub/mul/fma .rn.f32x2, sm_100a): one instruction per two sites, each
-// lane rounded exactly as the scalar operation.
-#define SP_F32X2_OP(NAME, OPC)                                                          \
-  __device__ __forceinline__ Vec<float, 2> NAME(const Vec<float, 2>& a, const Vec<float, 2>& b) { \
-    Vec<float, 2> r;                                                                    \
-    asm("{.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t" OPC      \
-        " d, a, b;\n\tmov.b64 {%0, %1}, d;}"                                             \
-        : "=f"(r.v[0]), "=f"(r.v[1])                                                    \
-        : "f"(a.v[0]), "f"(a.v[1]), "f"(b.v[0]), "f"(b.v[1]));                          \
-    return r;                                                                           \
-  }
-SP_F32X2_OP(operator+, "add.rn.f32x2")
-SP_F32X2_OP(operator-, "sub.rn.f32x2")
-SP_F32X2_OP(operator*, "mul.rn.f32x2")
-#undef SP_F32X2_OP
-
+// (__fadd2_rn / __fmul2_rn / __ffma2_rn, sm_100): one instruction per two
+// sites, each lane rounded exactly as the scalar operation (a - b is
+// a + (-b), which is exact).
+__device__ __forceinline__ float2 f2(const Vec<float, 2>& a) { return make_float2(a.v[0], a.v[1]); }
+__device__ __forceinline__ Vec<float, 2> v2(float2 a) {
+  Vec<float, 2> r;
+  r.v[0] = a.x;
+  r.v[1] = a.y;
+  return r;
+}
+__device__ __forceinline__ Vec<float, 2> operator+(const Vec<float, 2>& a, const Vec<float, 2>& b) {
+  return v2(__fadd2_rn(f2(a), f2(b)));
+}
+__device__ __forceinline__ Vec<float, 2> operator-(const Vec<float, 2>& a, const Vec<float, 2>& b) {
+  return v2(__fadd2_rn(f2(a), make_float2(-b.v[0], -b.v[1])));
+}
+__device__ __forceinline__ Vec<float, 2> operator*(const Vec<float, 2>& a, const Vec<float, 2>& b) {
+  return v2(__fmul2_rn(f2(a), f2(b)));
+}
 __device__ __forceinline__ Vec<float, 2> fma_op(const Vec<float, 2>& a, const Vec<float, 2>& b,
                                                  const Vec<float, 2>& c) {
-  Vec<float, 2> r;
-  asm("{.reg .b64 a, b, c, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
-      "mov.b64 c, {%6, %7};\n\tfma.rn.f32x2 d, a, b, c;\n\tmov.b64 {%0, %1}, d;}"
-      : "=f"(r.v[0]), "=f"(r.v[1])
-      : "f"(a.v[0]), "f"(a.v[1]), "f"(b.v[0]), "f"(b.v[1]), "f"(c.v[0]), "f"(c.v[1]));
-  return r;
+  return v2(__ffma2_rn(f2(a), f2(b), f2(c)));
 }
 __device__ __forceinline__ float fma_op(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_op(double a, double b, double c) { return __fma_rn(a, b, c); }

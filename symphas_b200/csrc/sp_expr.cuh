@@ -353,13 +353,28 @@ struct Ev<Pow<N, A>> {
     return rpow<N>(Ev<A>::template at<X, Y, Z>(e.a, c));
   }
 };
+// Laplacian in a context that may contract and reassociate (the fused form):
+// the 5- and 7-point sums become a balanced tree ending in one FMA, which
+// shortens the dependency chain; other point sets, and the exact form, keep
+// the reference's summation order.
 template <class A>
 struct Ev<Lap<A>> {
   template <int X, int Y, int Z, class C>
   __device__ __forceinline__ static typename C::value_type at(const Lap<A>& e, const C& c) {
     using T = typename C::value_type;
     Shifted<A, X, Y, Z, C> s{e.a, c};
-    return st::lap_pts<C::dim, C::lap_points>::template apply<T>(s, c.divh2);
+    if constexpr (C::contract && C::dim == 2 && C::lap_points == 5) {
+      const T sx = s.template at<-1, 0, 0>() + s.template at<1, 0, 0>();
+      const T sy = s.template at<0, -1, 0>() + s.template at<0, 1, 0>();
+      return fmadd<true>(T(-4.0) * c.divh2, s.template at<0, 0, 0>(), (sx + sy) * c.divh2);
+    } else if constexpr (C::contract && C::dim == 3 && C::lap_points == 7) {
+      const T sx = s.template at<-1, 0, 0>() + s.template at<1, 0, 0>();
+      const T sy = s.template at<0, -1, 0>() + s.template at<0, 1, 0>();
+      const T sz = s.template at<0, 0, -1>() + s.template at<0, 0, 1>();
+      return fmadd<true>(T(-6.0) * c.divh2, s.template at<0, 0, 0>(), ((sx + sy) + sz) * c.divh2);
+    } else {
+      return st::lap_pts<C::dim, C::lap_points>::template apply<T>(s, c.divh2);
+    }
   }
 };
 template <class A>

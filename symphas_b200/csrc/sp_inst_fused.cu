@@ -29,7 +29,9 @@
 #define SP_FUSED_VARIANTS3(MODEL, MF)                                                   \
   SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3b);        \
   SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3c);        \
-  SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3d);
+  SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3d);        \
+  SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3e);        \
+  SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3f);
 #define SP_FUSED_VARIANTS2(MODEL, MF0, MF1)                                             \
   SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2b);   \
   SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2c);
@@ -38,6 +40,13 @@ namespace sp {
 void register_fused_kernels() {
   SP_FUSED_SET(float, 0)
   SP_FUSED_SET(double, 1)
+  // conserved-pattern kernels (register z-queues) for models B and BMK
+  SP_REGCH3(SPK_B, MF_B_fused, ::sp::Tiles<float>::C3a);
+  SP_REGCH3(SPK_B, MF_B_fused, ::sp::Tiles<float>::C3b);
+  SP_REGCH3(SPK_B, MF_B_fused, ::sp::Tiles<float>::C3c);
+  SP_REGCH3(SPK_B, MF_B_fused, ::sp::Tiles<float>::C3d);
+  SP_REGCH3(SPK_BMK, MF_BMK_fused, ::sp::Tiles<float>::C3a);
+  SP_REGCH3(SPK_BMK, MF_BMK_fused, ::sp::Tiles<float>::C3c);
   SP_FUSED_VARIANTS3(SPK_A, MF_A_fused)
   SP_FUSED_VARIANTS3(SPK_B, MF_B_fused)
   SP_FUSED_VARIANTS3(SPK_C, MF_C_fused)

@@ -166,6 +166,38 @@ __device__ __forceinline__ void store_group(T* org, int x, int y, int z, const v
   }
 }
 
+// offset (in elements) of the periodic image of coordinate c along an axis of
+// length n and halo stride `stride`, or 0 when c is farther than R from both
+// faces; `w` is the width of the group stored at c
+__device__ __forceinline__ long long image_offset(int per, int c, int w, int n, int R,
+                                                  long long stride) {
+  if (!per) return 0;
+  if (c < R) return (long long)n * stride;
+  if (c + w > n - R) return -(long long)n * stride;
+  return 0;
+}
+
+// one vector store and its periodic images (x, y, z and their combinations);
+// the image offsets are 0 where there is no image
+template <class V, class T>
+__device__ __forceinline__ void put_images(T* p, const V& v, long long xo, long long yo,
+                                           long long zo) {
+  *reinterpret_cast<V*>(p) = v;
+  if (xo) *reinterpret_cast<V*>(p + xo) = v;
+  if (yo) {
+    *reinterpret_cast<V*>(p + yo) = v;
+    if (xo) *reinterpret_cast<V*>(p + yo + xo) = v;
+  }
+  if (zo) {
+    *reinterpret_cast<V*>(p + zo) = v;
+    if (xo) *reinterpret_cast<V*>(p + zo + xo) = v;
+    if (yo) {
+      *reinterpret_cast<V*>(p + zo + yo) = v;
+      if (xo) *reinterpret_cast<V*>(p + zo + yo + xo) = v;
+    }
+  }
+}
+
 // (s + d) mod N for 0 <= s < N and |d| < N, without a division
 template <int N>
 __device__ __forceinline__ int wrap(int s, int d) {
@@ -260,18 +292,27 @@ __global__ void __launch_bounds__(TC::NT)
   // output rows of this thread: pointers at plane 0 and which need halo images
   const int x = x0 + txt * W;
   const bool xin = x < p.n[0];
-  const bool xedge = (p.per[0] && (x < R || x + W > p.n[0] - R)) || (x + W > p.n[0]);
+  // whole W-groups (every group but a ragged row end) store as vectors, their
+  // periodic images too
+  const bool vec_ok = (p.n[0] % W == 0) && (x + W <= p.n[0]);
+  const long long xo = image_offset(p.per[0], x, W, p.n[0], R, 1);
   T* orow[SPT][NF];
-  bool rowin[SPT], rowedge[SPT];
+  bool rowin[SPT];
+  long long yo[SPT];
+  // `simple`: every row of this thread is inside, stores whole vectors and has
+  // no x or y image -- its stores are then straight-line code
+  bool simple = vec_ok && xo == 0;
 #pragma unroll
   for (int k = 0; k < SPT; ++k) {
     const int y = y0 + row0 + k;
     rowin[k] = xin && y < p.n[1];
-    rowedge[k] = xedge || (p.per[1] && (y < R || y >= p.n[1] - R));
+    yo[k] = image_offset(p.per[1], y, 1, p.n[1], R, p.pitch);
+    simple = simple && rowin[k] && yo[k] == 0;
 #pragma unroll
     for (int f = 0; f < NF; ++f)
       orow[k][f] = p.out[inst * NF + f] + (long long)(y + p.h[1]) * p.pitch + (x + p.h[0]);
   }
+  const bool do_mass = p.partial != nullptr;
   // the stage cell beyond this thread's row groups, if any
   int xsr = -1, xsc = 0;
   if constexpr (NS > 0) {
@@ -310,7 +351,6 @@ __global__ void __launch_bounds__(TC::NT)
   }
 
   double msum = 0.0;
-  int waited = -1;
   // ring slot of plane zi (field ring) and of staged plane zi (stage ring),
   // advanced by one per iteration instead of divided out
   int zslot = ((zi0 - (zb - R)) % NSLOT + NSLOT) % NSLOT;
@@ -322,8 +362,11 @@ __global__ void __launch_bounds__(TC::NT)
     if (tid == 0 && qn < nplanes) issue(qn);
     bool bad = false;
     const int qw = zi + U - (zb - R);
-    for (int q = waited + 1; q <= qw; ++q) bad |= !tma::mbar_wait(&bars[q % NSLOT], (q / NSLOT) & 1);
-    waited = qw;
+    if (zi == zi0) {
+      for (int q = 0; q <= qw; ++q) bad |= !tma::mbar_wait(&bars[q % NSLOT], (q / NSLOT) & 1);
+    } else {
+      bad = !tma::mbar_wait(&bars[wrap<NSLOT>(zslot, U)], (qw / NSLOT) & 1);
+    }
 
     if constexpr (NS > 0) {
       using CS = Ctx<T, W, !EXACT, 3, LP, GP, BP, NF, 2 * RI + 1, RI, PW, 1, 1, 0, SW>;
@@ -417,20 +460,31 @@ __global__ void __launch_bounds__(TC::NT)
         }
       }
       const long long zoff = (long long)(z + p.h[2]) * p.plane;
-      const bool zedge = p.per[2] && (z < R || z >= p.n[2] - R);
+      const long long zo = image_offset(p.per[2], z, 1, p.n[2], R, p.plane);
+      if (simple && zo == 0) {
 #pragma unroll
-      for (int k = 0; k < SPT; ++k) {
-        if (!rowin[k]) continue;
-        if (!(rowedge[k] || zedge)) {
+        for (int k = 0; k < SPT; ++k)
 #pragma unroll
           for (int f = 0; f < NF; ++f) *reinterpret_cast<V*>(orow[k][f] + zoff) = nv[k][f];
-        } else {
+      } else {
 #pragma unroll
-          for (int f = 0; f < NF; ++f)
-            store_group<T, W, 3, R>(p.out[inst * NF + f], x, y0 + row0 + k, z, nv[k][f], p.n,
-                                    p.h, p.per, p.pitch, p.plane);
+        for (int k = 0; k < SPT; ++k) {
+          if (!rowin[k]) continue;
+          if (vec_ok) {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) put_images(orow[k][f] + zoff, nv[k][f], xo, yo[k], zo);
+          } else {
+#pragma unroll
+            for (int f = 0; f < NF; ++f)
+              store_group<T, W, 3, R>(p.out[inst * NF + f], x, y0 + row0 + k, z, nv[k][f], p.n,
+                                      p.h, p.per, p.pitch, p.plane);
+          }
         }
-        if (p.partial) msum += vsum<T, W>(nv[k][0], x, p.n[0]);
+      }
+      if (do_mass) {
+#pragma unroll
+        for (int k = 0; k < SPT; ++k)
+          if (rowin[k]) msum += vsum<T, W>(nv[k][0], x, p.n[0]);
       }
     }
   }
@@ -569,25 +623,46 @@ __device__ __forceinline__ void fd2_out(const Step2Params<T>& p, const M& m, con
       nv[k][1] = p.rhs_only ? r1 : fmadd<!K::exact>(vdt, r1, ctx.template var<2, 0, 0, 0>());
     }
   }
-  const bool xedge = (ip.per[0] && (x < R || x + W > n0 - R)) || (x + W > n0);
+  const bool vec_ok = (n0 % W == 0) && (x + W <= n0);
+  const long long xo = image_offset(ip.per[0], x, W, n0, R, 1);
   const int h[3] = {p.hx, p.hy, 0};
   const int n3[3] = {n0, n1, 1};
   const int per3[3] = {ip.per[0], ip.per[1], 0};
+  T* out[NF];
 #pragma unroll
-  for (int k = 0; k < SPT; ++k) {
-    const int y = y0 + row0 + k;
-    if (x >= n0 || y >= n1) continue;
-    if (!(xedge || (ip.per[1] && (y < R || y >= n1 - R)))) {
+  for (int f = 0; f < NF; ++f) out[f] = p.out[ii * NF + f];
+  const int yr0 = y0 + row0;
+  const bool simple = vec_ok && xo == 0 && yr0 + SPT <= n1 &&
+                      !(ip.per[1] && (yr0 < R || yr0 + SPT > n1 - R));
+  if (simple) {
+    T* b0 = nullptr;
 #pragma unroll
-      for (int f = 0; f < NF; ++f)
-        *reinterpret_cast<V*>(p.out[ii * NF + f] + (long long)(y + p.hy) * pitch + x + p.hx) =
-            nv[k][f];
-    } else {
+    for (int f = 0; f < NF; ++f) {
+      b0 = out[f] + (long long)(yr0 + p.hy) * pitch + x + p.hx;
 #pragma unroll
-      for (int f = 0; f < NF; ++f)
-        store_group<T, W, 2, R>(p.out[ii * NF + f], x, y, 0, nv[k][f], n3, h, per3, pitch, 0);
+      for (int k = 0; k < SPT; ++k) *reinterpret_cast<V*>(b0 + k * pitch) = nv[k][f];
     }
-    if (p.partial) msum += vsum<T, W>(nv[k][0], x, n0);
+  } else {
+#pragma unroll
+    for (int k = 0; k < SPT; ++k) {
+      const int y = y0 + row0 + k;
+      if (x >= n0 || y >= n1) continue;
+      if (vec_ok) {
+        const long long yo = image_offset(ip.per[1], y, 1, n1, R, pitch);
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+          put_images(out[f] + (long long)(y + p.hy) * pitch + x + p.hx, nv[k][f], xo, yo, 0LL);
+      } else {
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+          store_group<T, W, 2, R>(out[f], x, y, 0, nv[k][f], n3, h, per3, pitch, 0);
+      }
+    }
+  }
+  if (p.partial) {
+#pragma unroll
+    for (int k = 0; k < SPT; ++k)
+      if (x < n0 && y0 + row0 + k < n1) msum += vsum<T, W>(nv[k][0], x, n0);
   }
 }
 

@@ -3,6 +3,7 @@
  */
 #pragma once
 
+#include "sp_ch.cuh"
 #include "sp_kernels.cuh"
 #include "sp_models.cuh"
 #include "sp_registry.h"
@@ -36,6 +37,34 @@ struct Entry3 {
   static KernelInfo info() {
     return KernelInfo{K::NF, K::NS,     K::R,    K::HXA,  K::TX,      K::TY,
                       K::SPT, K::PD, K::NT, K::SMEM, &launch, &occupancy};
+  }
+};
+
+// the conserved-pattern kernel (sp_ch.cuh) as a tile variant of a fused key
+template <class MF, class T, class TC>
+struct EntryCh3 {
+  using M = model_of<MF>;
+  using K = Ch3<M, T, TC>;
+  static cudaError_t launch(const void* prm, dim3 grid, cudaStream_t s) {
+    auto kern = k_ch3d<M, T, TC>;
+    static cudaError_t attr = cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
+    if (attr != cudaSuccess) return attr;
+    const M m = MF{}();
+    kern<<<grid, K::NT, K::SMEM, s>>>(*static_cast<const StepParams<T>*>(prm), m);
+    return cudaGetLastError();
+  }
+  static int occupancy() {
+    auto kern = k_ch3d<M, T, TC>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, K::NT, K::SMEM) != cudaSuccess)
+      return 1;
+    return n > 0 ? n : 1;
+  }
+  static KernelInfo info() {
+    return KernelInfo{1, 1, K::R, K::HXA, K::TX, K::TY, K::SPT, K::PD, K::NT, K::SMEM,
+                      &launch, &occupancy};
   }
 };
 
@@ -115,6 +144,12 @@ template <> struct Tiles<float> {
   using D3b = TileCfg<64, 32, 4, 2, 2>;
   using D3c = TileCfg<64, 16, 4, 4, 2>;
   using D3d = TileCfg<128, 16, 4, 2, 2>;
+  using D3e = TileCfg<64, 16, 2, 2, 2>;
+  using D3f = TileCfg<64, 16, 4, 2, 2>;
+  using C3a = TileCfg<64, 16, 4, 2, 2>;  // conserved-pattern kernel shapes
+  using C3b = TileCfg<64, 16, 2, 2, 2>;
+  using C3c = TileCfg<64, 32, 4, 2, 2>;
+  using C3d = TileCfg<128, 16, 4, 2, 2>;
   using D2b = TileCfg<64, 32, 4, 3, 2>;
   using D2c = TileCfg<128, 32, 8, 2, 2>;
 };
@@ -133,6 +168,9 @@ template <> struct Tiles<double> {
 #define SP_REG3T(MODEL, FORM, MF, T, DT, LP, GP, BP, TILE)                  \
   ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 3, DT, LP, GP, BP},    \
                         ::sp::Entry3<::sp::MF, T, LP, GP, BP, TILE, FORM == SPK_EXACT>::info())
+#define SP_REGCH3(MODEL, MF, TILE)                                          \
+  ::sp::register_kernel(::sp::KernelKey{MODEL, SPK_FUSED, 3, 0, 7, 10, 25},  \
+                        ::sp::EntryCh3<::sp::MF, float, TILE>::info())
 #define SP_REG2T(MODEL, FORM, MF0, MF1, T, DT, LP, GP, BP, TILE)            \
   ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 2, DT, LP, GP, BP},    \
                         ::sp::Entry2<::sp::MF0, ::sp::MF1, T, LP, GP, BP, TILE, FORM == SPK_EXACT>::info())

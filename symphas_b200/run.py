@@ -27,6 +27,8 @@ def main(argv=None):
     ap.add_argument("--dt", type=float, default=0.005)
     ap.add_argument("--h", type=float, default=1.0)
     ap.add_argument("--coeff", type=float, nargs="*", default=[])
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick the fastest tile shape first (its launches come before the steps)")
     a = ap.parse_args(argv)
     st = sp.Stencil2d2h(5, 6, 13) if a.dim == 2 else sp.Stencil3d2h(7, 10, 25)
     cls = MODELS[a.model]
@@ -36,6 +38,7 @@ def main(argv=None):
     m.fill_uniform(0, 1, -0.3, -0.1)
     if cls.nfields > 1:
         m.fill_uniform(1, 2, -0.1, 0.1)
+    info = m.autotune(5) if a.autotune else m.kernel_info()
     m.synchronize()
     t0 = time.perf_counter()
     for _ in range(a.steps):
@@ -44,7 +47,7 @@ def main(argv=None):
     el = time.perf_counter() - t0
     print(json.dumps({"model": a.model, "dim": a.dim, "n": a.n, "dtype": a.dtype, "form": a.form,
                       "steps": a.steps, "wall_ms_per_step": 1e3 * el / a.steps,
-                      "launches": m.launch_count()}))
+                      "launches": m.launch_count(), "kernel": info}))
     m.close()
 
 
