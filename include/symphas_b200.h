@@ -99,6 +99,34 @@ typedef struct sp_handle sp_handle;
  * (interior + halo, ping-pong) and builds the TMA descriptors. */
 int sp_create(const sp_desc* desc, sp_handle** out);
 
+/* ---- ensembles of independent 2D systems --------------------------------
+ * One member of an ensemble: its own interior extents (x, y; n[2] unused),
+ * model (SP_MODEL_*), time step and coefficients c(1)..c(8).  SymPhas runs
+ * such a sweep as one Model object per member, stepped one after another by
+ * find_solution (modules-io.h:747-753); here every member advances in the same
+ * persistent kernel launch, which takes (member, tile) work items from one
+ * queue, so small and large members share the GPU without a launch each. */
+typedef struct sp_member {
+  int n[3];
+  int model;
+  double dt;
+  double coeff[8];
+} sp_member;
+
+/* model id reported for an ensemble that mixes SP_MODEL_AMK and SP_MODEL_BMK
+ * members (one kernel holding both right-hand sides) */
+#define SP_ENSEMBLE_AMK_BMK 5
+
+/* Create a handle over `count` members.  `desc` gives what they share: dim
+ * (must be 2), dtype, form, stencil point counts, boundaries and h; its n,
+ * model, dt, coeff and batch are ignored.  The members either all have one
+ * model, or mix SP_MODEL_AMK and SP_MODEL_BMK.  Instance i of the handle is
+ * member i: sp_upload, sp_download, sp_fill_uniform, sp_reduce and
+ * sp_field_geometry take its own extents; sp_step advances every member by
+ * its own dt; sp_set_dt is rejected. */
+int sp_create_ensemble(const sp_desc* desc, const sp_member* members, int count,
+                       sp_handle** out);
+
 /* Copy `bytes` of interior values (x-fastest, dtype of the handle) of field
  * `field` of instance `inst` from host memory, then refresh its halo. */
 int sp_upload(sp_handle* h, int inst, int field, const void* host, size_t bytes);

@@ -17,6 +17,7 @@ SP_PERIODIC, SP_DIRICHLET = 0, 1
 SP_MODEL_A, SP_MODEL_B, SP_MODEL_C, SP_MODEL_AMK, SP_MODEL_BMK = 0, 1, 2, 3, 4
 SP_OP_LAP, SP_OP_BILAP, SP_OP_GRADLAP, SP_OP_LAPCUBE = 10, 11, 12, 13
 SP_FORM_EXACT, SP_FORM_FUSED = 1, 0
+SP_ENSEMBLE_AMK_BMK = 5
 SP_NOALLOC_MAX_INSTANCES = 64
 
 _STATUS = {
@@ -56,6 +57,15 @@ class SpDesc(ctypes.Structure):
     ]
 
 
+class SpMember(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int * 3),
+        ("model", ctypes.c_int),
+        ("dt", ctypes.c_double),
+        ("coeff", ctypes.c_double * 8),
+    ]
+
+
 _H = ctypes.c_void_p
 _P = ctypes.c_void_p
 _SZ = ctypes.c_size_t
@@ -63,6 +73,8 @@ _SZ = ctypes.c_size_t
 # name -> (restype, argtypes); every function declared in include/symphas_b200.h
 SIGNATURES = {
     "sp_create": (ctypes.c_int, [ctypes.POINTER(SpDesc), ctypes.POINTER(_H)]),
+    "sp_create_ensemble": (ctypes.c_int, [ctypes.POINTER(SpDesc), ctypes.POINTER(SpMember),
+                                          ctypes.c_int, ctypes.POINTER(_H)]),
     "sp_upload": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _P, _SZ]),
     "sp_upload_device": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _P, _SZ]),
     "sp_fill_uniform": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,

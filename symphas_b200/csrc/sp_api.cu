@@ -82,13 +82,30 @@ __global__ void k_seed(T* org, int dim, int n0, int n1, int n2, int h0, int h1, 
 // ---------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------
+// geometry and parameters of one instance: every instance of a batch has the
+// same, the members of an ensemble each their own
+struct InstGeo {
+  int n[3] = {1, 1, 1};
+  long long pitch = 0, ly = 0, lz = 1, plane = 0, felems = 0;
+  size_t off = 0;  // element offset of the instance's field 0 in each buffer
+  int model = 0;   // SP_MODEL_* of the instance
+  int kind = 0;    // 0 = first model of the kernel, 1 = second (ensembles)
+  double dt = 0.0;
+  double coeff[8] = {1, 1, 1, 1, 1, 1, 1, 1};
+  long long sites() const { return (long long)n[0] * n[1] * n[2]; }
+};
+
 struct sp_handle {
   sp_desc d{};
+  std::vector<InstGeo> geo;  // [batch]
+  bool ensemble = false;     // members differ in size, model or parameters
   const sp::KernelInfo* ki = nullptr;   // the chosen tile variant
   std::vector<sp::KernelInfo> variants;  // every tile shape built for this kernel
   int variant = 0;
   int nf = 1, batch = 1, dim = 2;
-  int n[3] = {1, 1, 1}, h[3] = {0, 0, 0};
+  int h[3] = {0, 0, 0};  // halo of every instance
+  // geometry of instance 0 (the geometry of every instance of a 3D batch)
+  int n[3] = {1, 1, 1};
   long long pitch = 0, ly = 0, lz = 1, plane = 0, felems = 0;
   size_t esz = 8;
   char* buf[2] = {nullptr, nullptr};
@@ -167,11 +184,25 @@ int energy_kind(int model) {
 }
 
 char* field_base(sp_handle* H, int which, int inst, int f) {
-  return H->buf[which] + size_t(inst * H->nf + f) * H->felems * H->esz;
+  const InstGeo& g = H->geo[inst];
+  return H->buf[which] + (g.off + size_t(f) * g.felems) * H->esz;
 }
 char* field_origin(sp_handle* H, int which, int inst, int f) {
+  const InstGeo& g = H->geo[inst];
   return field_base(H, which, inst, f) +
-         size_t((H->dim == 3 ? H->h[2] : 0) * H->plane + H->h[1] * H->pitch + H->h[0]) * H->esz;
+         size_t((H->dim == 3 ? H->h[2] : 0) * g.plane + H->h[1] * g.pitch + H->h[0]) * H->esz;
+}
+
+// padded layout of an instance of extents n: x padded to whole 16-byte units
+// past the halo, each field rounded up to 64 elements (256 or 512 bytes)
+void set_geometry(sp_handle* H, InstGeo& g, const int n[3]) {
+  for (int a = 0; a < 3; ++a) g.n[a] = (a < H->dim) ? n[a] : 1;
+  const int va = int(16 / H->esz);
+  g.pitch = ((g.n[0] + 2 * H->h[0] + va - 1) / va) * va;
+  g.ly = g.n[1] + 2 * H->h[1];
+  g.lz = H->dim == 3 ? g.n[2] + 2 * H->h[2] : 1;
+  g.plane = g.pitch * g.ly;
+  g.felems = ((g.plane * g.lz + 63) / 64) * 64;
 }
 
 int check_err_flag(sp_handle* H) {
@@ -180,6 +211,8 @@ int check_err_flag(sp_handle* H) {
   SP_CUDA(H, cudaStreamSynchronize(H->stream));
   if (e != 0) {
     cudaMemsetAsync(H->err_d, 0, sizeof(int), H->stream);
+    // a CTA that gave up left the 2D work queue without re-arming it
+    if (H->ctr_d) cudaMemsetAsync(H->ctr_d, 0, 2 * sizeof(int), H->stream);
     return fail(H, SP_ETIMEOUT, "a kernel gave up waiting for a TMA tile (device error flag set)");
   }
   return SP_OK;
@@ -242,15 +275,16 @@ int launch_step(sp_handle* H, int rhs_only, double* partial) {
 
 template <class T>
 int fill_halo_t(sp_handle* H, int which, int inst, int f) {
+  const InstGeo& g = H->geo[inst];
   sp::HaloParams<T> p{};
   p.org = reinterpret_cast<T*>(field_base(H, which, inst, f));
   p.dim = H->dim;
   for (int a = 0; a < 3; ++a) {
-    p.n[a] = H->n[a];
+    p.n[a] = g.n[a];
     p.h[a] = H->h[a];
   }
-  p.pitch = H->pitch;
-  p.plane = H->plane;
+  p.pitch = g.pitch;
+  p.plane = g.plane;
   for (int s = 0; s < 6; ++s) {
     p.bc[s] = H->d.boundary[s];
     p.bv[s] = T(H->d.boundary_value[s]);
@@ -316,20 +350,22 @@ int setup_2d_t(sp_handle* H) {
   std::vector<sp::Inst2<T>> ip(H->batch);
   const double divh = 1.0 / H->d.h;
   const double divh2 = divh * divh, divh3 = divh * divh2, divh4 = divh2 * divh2;
+  const int tx = H->ki->tx, ty = H->ki->ty;
   for (int i = 0; i < H->batch; ++i) {
+    const InstGeo& g = H->geo[i];
     sp::Inst2<T>& q = ip[i];
-    q.n[0] = H->n[0];
-    q.n[1] = H->n[1];
+    q.n[0] = g.n[0];
+    q.n[1] = g.n[1];
     q.per[0] = H->d.boundary[0] == SP_PERIODIC;
     q.per[1] = H->d.boundary[2] == SP_PERIODIC;
-    q.pitch = H->pitch;
-    q.ntx = H->ntx;
-    q.kind = 0;
-    q.dt = T(H->d.dt);
+    q.pitch = g.pitch;
+    q.ntx = (g.n[0] + tx - 1) / tx;
+    q.kind = g.kind;
+    q.dt = T(g.dt);
     q.divh2 = T(divh2);
     q.divh3 = T(divh3);
     q.divh4 = T(divh4);
-    for (int c = 0; c < 8; ++c) q.coef[c] = T(H->d.coeff[c]);
+    for (int c = 0; c < 8; ++c) q.coef[c] = T(g.coeff[c]);
   }
   cudaFree(H->inst2_d);
   cudaFree(H->items_d);
@@ -338,12 +374,26 @@ int setup_2d_t(sp_handle* H) {
   SP_CUDA(H, cudaMalloc(&H->inst2_d, sizeof(sp::Inst2<T>) * H->batch));
   SP_CUDA(H, cudaMemcpy(H->inst2_d, ip.data(), sizeof(sp::Inst2<T>) * H->batch,
                         cudaMemcpyHostToDevice));
-  const int tiles = H->ntx * H->nty;
-  H->nitems = tiles * H->batch;
+  // work items (instance, tile); the persistent CTAs take them in this order,
+  // so the costlier ones go first (the second model of an ensemble stages an
+  // operand, and larger instances hold more tiles) and the cheap ones fill
+  // the tail of the step
+  std::vector<int> order(H->batch);
+  for (int i = 0; i < H->batch; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    const InstGeo &gx = H->geo[x], &gy = H->geo[y];
+    if (gx.kind != gy.kind) return gx.kind > gy.kind;
+    return gx.sites() > gy.sites();
+  });
+  std::vector<int2> items;
+  for (int i : order) {
+    const int tiles = ip[i].ntx * ((H->geo[i].n[1] + ty - 1) / ty);
+    for (int t = 0; t < tiles; ++t) items.push_back(make_int2(i, t));
+  }
+  H->nitems = int(items.size());
+  H->ntx = ip[0].ntx;
+  H->nty = (H->geo[0].n[1] + ty - 1) / ty;
   if (H->batch > 1) {
-    std::vector<int2> items(H->nitems);
-    for (int i = 0; i < H->batch; ++i)
-      for (int t = 0; t < tiles; ++t) items[size_t(i) * tiles + t] = make_int2(i, t);
     SP_CUDA(H, cudaMalloc(&H->items_d, sizeof(int2) * items.size()));
     SP_CUDA(H, cudaMemcpy(H->items_d, items.data(), sizeof(int2) * items.size(),
                           cudaMemcpyHostToDevice));
@@ -382,6 +432,7 @@ int configure(sp_handle* H, int variant) {
     for (int i = 0; i < H->batch; ++i)
       for (int f = 0; f < H->nf; ++f) {
         const int idx = i * H->nf + f;
+        const InstGeo& g = H->geo[i];
         void* base = field_base(H, k, i, f);
         outs[idx] = base;
         const cuuint32_t bw = cuuint32_t(H->ki->tx + 2 * H->h[0]);
@@ -390,16 +441,16 @@ int configure(sp_handle* H, int variant) {
             H->esz == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
         CUresult r;
         if (H->dim == 3) {
-          cuuint64_t gdim[3] = {cuuint64_t(H->pitch), cuuint64_t(H->ly), cuuint64_t(H->lz)};
-          cuuint64_t gstr[2] = {cuuint64_t(H->pitch * H->esz), cuuint64_t(H->plane * H->esz)};
+          cuuint64_t gdim[3] = {cuuint64_t(g.pitch), cuuint64_t(g.ly), cuuint64_t(g.lz)};
+          cuuint64_t gstr[2] = {cuuint64_t(g.pitch * H->esz), cuuint64_t(g.plane * H->esz)};
           cuuint32_t box[3] = {bw, bh, 1};
           cuuint32_t es[3] = {1, 1, 1};
           r = enc(&maps[idx], dt, 3, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         } else {
-          cuuint64_t gdim[2] = {cuuint64_t(H->pitch), cuuint64_t(H->ly)};
-          cuuint64_t gstr[1] = {cuuint64_t(H->pitch * H->esz)};
+          cuuint64_t gdim[2] = {cuuint64_t(g.pitch), cuuint64_t(g.ly)};
+          cuuint64_t gstr[1] = {cuuint64_t(g.pitch * H->esz)};
           cuuint32_t box[2] = {bw, bh};
           cuuint32_t es[2] = {1, 1};
           r = enc(&maps[idx], dt, 2, base, gdim, gstr, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -459,44 +510,98 @@ std::tuple<int, int, int, int, int, int, int, int, int, int, int> tune_key(const
           H->n[0], H->n[1], H->n[2], H->batch};
 }
 
-int create(const sp_desc* desc, sp_handle* H) {
+// kernel model of an ensemble: one model shared by every member, or the
+// two-model kernel for members of models AMK and BMK (kind 0 and 1)
+int ensemble_model(const sp_member* m, int count, std::string& why) {
+  bool amk = false, bmk = false, same = true;
+  for (int i = 0; i < count; ++i) {
+    same = same && m[i].model == m[0].model;
+    amk = amk || m[i].model == SP_MODEL_AMK;
+    bmk = bmk || m[i].model == SP_MODEL_BMK;
+  }
+  if (same) return m[0].model;
+  for (int i = 0; i < count; ++i)
+    if (m[i].model != SP_MODEL_AMK && m[i].model != SP_MODEL_BMK)
+      return why = "an ensemble mixes models only of SP_MODEL_AMK and SP_MODEL_BMK", -1;
+  return SP_ENSEMBLE_AMK_BMK;
+}
+
+// a handle over `desc` (a batch of identical instances), or, when `members`
+// is given, over `count` members that each have their own extents, model,
+// time step and coefficients (desc then supplies dim, dtype, form, stencil,
+// boundaries and h)
+int create(const sp_desc* desc, const sp_member* members, int count, sp_handle* H) {
   std::string why;
-  if (int rc = validate(desc, why)) return fail(H, rc, why);
+  sp_desc dd{};
+  if (desc) dd = *desc;
+  if (members) {
+    if (!desc) return fail(H, SP_EINVAL, "null description");
+    if (count < 1) return fail(H, SP_EINVAL, "an ensemble needs at least one member");
+    if (desc->dim != 2) return fail(H, SP_EINVAL, "ensembles are two-dimensional");
+    for (int i = 0; i < count; ++i) {
+      for (int a = 0; a < 2; ++a)
+        if (members[i].n[a] < 4 || members[i].n[a] > (1 << 16))
+          return fail(H, SP_EINVAL, "each extent must be in [4, 65536]");
+      if (!std::isfinite(members[i].dt)) return fail(H, SP_EINVAL, "dt must be finite");
+    }
+    const int model = ensemble_model(members, count, why);
+    if (model < 0) return fail(H, SP_EINVAL, why);
+    dd.model = model;
+    dd.n[0] = members[0].n[0];
+    dd.n[1] = members[0].n[1];
+    dd.batch = count;
+    dd.dt = members[0].dt;
+    for (int c = 0; c < 8; ++c) dd.coeff[c] = members[0].coeff[c];
+    H->ensemble = true;
+  }
+  if (int rc = validate(desc ? &dd : nullptr, why)) return fail(H, rc, why);
   sp::register_all_kernels();
-  H->d = *desc;
-  H->dim = desc->dim;
-  H->batch = desc->batch;
-  H->esz = desc->dtype == SP_F32 ? 4 : 8;
-  const sp::KernelKey key{desc->model, desc->form, desc->dim, desc->dtype,
-                          desc->lap_pts, desc->gradlap_pts, desc->bilap_pts};
+  H->d = dd;
+  H->dim = dd.dim;
+  H->batch = dd.batch;
+  H->esz = dd.dtype == SP_F32 ? 4 : 8;
+  const sp::KernelKey key{dd.model, dd.form, dd.dim, dd.dtype,
+                          dd.lap_pts, dd.gradlap_pts, dd.bilap_pts};
   const std::vector<sp::KernelInfo>* vs = sp::find_kernels(key);
   if (!vs || vs->empty()) {
     char b[256];
     snprintf(b, sizeof b,
              "no fused kernel built for model %d form %d dim %d dtype %d stencil <%d,%d,%d>",
-             desc->model, desc->form, desc->dim, desc->dtype, desc->lap_pts,
-             desc->gradlap_pts, desc->bilap_pts);
+             dd.model, dd.form, dd.dim, dd.dtype, dd.lap_pts, dd.gradlap_pts, dd.bilap_pts);
     return fail(H, SP_EINVAL, b);
   }
   H->variants = *vs;
   H->ki = &H->variants[0];
   H->nf = H->ki->nf;
-  for (int a = 0; a < 3; ++a) H->n[a] = (a < H->dim) ? desc->n[a] : 1;
   const int R = H->ki->R;
-  for (int a = 0; a < H->dim; ++a)
-    if (H->n[a] < 2 * R) return fail(H, SP_EINVAL, "an extent is smaller than twice the stencil reach");
   H->h[0] = H->ki->hx;
   H->h[1] = R;
   H->h[2] = H->dim == 3 ? R : 0;
   for (const sp::KernelInfo& v : H->variants)
     if (v.hx != H->h[0] || v.R != R || v.nf != H->nf)
       return fail(H, SP_EINVAL, "tile variants of one kernel disagree on the halo");
-  const int va = int(16 / H->esz);
-  H->pitch = ((H->n[0] + 2 * H->h[0] + va - 1) / va) * va;
-  H->ly = H->n[1] + 2 * H->h[1];
-  H->lz = H->dim == 3 ? H->n[2] + 2 * H->h[2] : 1;
-  H->plane = H->pitch * H->ly;
-  H->felems = ((H->plane * H->lz + 63) / 64) * 64;
+  H->geo.resize(H->batch);
+  size_t off = 0;
+  for (int i = 0; i < H->batch; ++i) {
+    InstGeo& g = H->geo[i];
+    set_geometry(H, g, members ? members[i].n : dd.n);
+    for (int a = 0; a < H->dim; ++a)
+      if (g.n[a] < 2 * R)
+        return fail(H, SP_EINVAL, "an extent is smaller than twice the stencil reach");
+    g.off = off;
+    off += size_t(H->nf) * g.felems;
+    g.model = members ? members[i].model : dd.model;
+    g.kind = (dd.model == SP_ENSEMBLE_AMK_BMK && g.model == SP_MODEL_BMK) ? 1 : 0;
+    g.dt = members ? members[i].dt : dd.dt;
+    for (int c = 0; c < 8; ++c) g.coeff[c] = members ? members[i].coeff[c] : dd.coeff[c];
+  }
+  const InstGeo& g0 = H->geo[0];
+  for (int a = 0; a < 3; ++a) H->n[a] = g0.n[a];
+  H->pitch = g0.pitch;
+  H->ly = g0.ly;
+  H->lz = g0.lz;
+  H->plane = g0.plane;
+  H->felems = g0.felems;
 
   int dev = 0;
   SP_CUDA(H, cudaGetDevice(&dev));
@@ -504,7 +609,7 @@ int create(const sp_desc* desc, sp_handle* H) {
   SP_CUDA(H, cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking));
   H->own_stream = true;
 
-  const size_t bytes = size_t(H->batch) * H->nf * H->felems * H->esz;
+  const size_t bytes = off * H->esz;
   for (int k = 0; k < 2; ++k) {
     if (cudaMalloc(&H->buf[k], bytes) != cudaSuccess)
       return fail(H, SP_ENOMEM, "device allocation of the field buffers failed");
@@ -518,7 +623,7 @@ int create(const sp_desc* desc, sp_handle* H) {
   // tile shape: an explicit choice (SP_TILE), else the one sp_autotune found
   // for this kernel and size in this process, else the first registered
   int variant = 0;
-  {
+  if (!H->ensemble) {
     std::lock_guard<std::mutex> lk(g_tune_mutex);
     auto it = g_tuned.find(tune_key(H));
     if (it != g_tuned.end()) variant = it->second;
@@ -534,17 +639,18 @@ int check_field(sp_handle* H, int inst, int field, size_t bytes) {
   if (!H) return SP_EINVAL;
   if (inst < 0 || inst >= H->batch) return fail(H, SP_EINVAL, "instance index out of range");
   if (field < 0 || field >= H->nf) return fail(H, SP_EINVAL, "field index out of range");
-  const size_t need = size_t(H->n[0]) * H->n[1] * (H->dim == 3 ? H->n[2] : 1) * H->esz;
+  const size_t need = size_t(H->geo[inst].sites()) * H->esz;
   if (bytes != need) return fail(H, SP_EINVAL, "byte count does not match the interior size");
   return SP_OK;
 }
 
 cudaMemcpy3DParms interior_copy(sp_handle* H, int which, int inst, int field, void* other,
                                 bool to_device, cudaMemcpyKind kind) {
+  const InstGeo& g = H->geo[inst];
   cudaMemcpy3DParms p{};
-  cudaPitchedPtr dev = make_cudaPitchedPtr(field_base(H, which, inst, field), H->pitch * H->esz,
-                                           H->pitch, H->ly);
-  cudaPitchedPtr com = make_cudaPitchedPtr(other, H->n[0] * H->esz, H->n[0], H->n[1]);
+  cudaPitchedPtr dev = make_cudaPitchedPtr(field_base(H, which, inst, field), g.pitch * H->esz,
+                                           g.pitch, g.ly);
+  cudaPitchedPtr com = make_cudaPitchedPtr(other, g.n[0] * H->esz, g.n[0], g.n[1]);
   cudaPos dpos = make_cudaPos(H->h[0] * H->esz, H->h[1], H->dim == 3 ? H->h[2] : 0);
   if (to_device) {
     p.srcPtr = com;
@@ -555,7 +661,7 @@ cudaMemcpy3DParms interior_copy(sp_handle* H, int which, int inst, int field, vo
     p.srcPos = dpos;
     p.dstPtr = com;
   }
-  p.extent = make_cudaExtent(H->n[0] * H->esz, H->n[1], H->dim == 3 ? H->n[2] : 1);
+  p.extent = make_cudaExtent(g.n[0] * H->esz, g.n[1], g.n[2]);
   p.kind = kind;
   return p;
 }
@@ -604,25 +710,26 @@ int capture_graph(sp_handle* H) {
 
 template <class T>
 int reduce_t(sp_handle* H, int inst, int field, double* mass, double* energy) {
+  const InstGeo& g = H->geo[inst];
   sp::ReduceParams<T> p{};
   p.f0 = reinterpret_cast<const T*>(field_base(H, H->cur, inst, field));
   p.e0 = reinterpret_cast<const T*>(field_base(H, H->cur, inst, 0));
   p.e1 = H->nf > 1 ? reinterpret_cast<const T*>(field_base(H, H->cur, inst, 1)) : nullptr;
   p.dim = H->dim;
   for (int a = 0; a < 3; ++a) {
-    p.n[a] = H->n[a];
+    p.n[a] = g.n[a];
     p.h[a] = H->h[a];
   }
-  p.pitch = H->pitch;
-  p.plane = H->plane;
-  p.energy_kind = energy_kind(H->d.model);
-  p.c1 = H->d.coeff[0];
-  p.c2 = H->d.coeff[1];
-  p.kappa = H->d.model == SP_MODEL_C ? 1.0 : H->d.coeff[1];
-  p.gamma = H->d.coeff[0];
+  p.pitch = g.pitch;
+  p.plane = g.plane;
+  p.energy_kind = energy_kind(g.model);
+  p.c1 = g.coeff[0];
+  p.c2 = g.coeff[1];
+  p.kappa = g.model == SP_MODEL_C ? 1.0 : g.coeff[1];
+  p.gamma = g.coeff[0];
   p.h_sp = H->d.h;
   p.partial = H->partial_d;
-  const long long total = (long long)H->n[0] * H->n[1] * (H->dim == 3 ? H->n[2] : 1);
+  const long long total = g.sites();
   int blocks = int(std::min<long long>((total + RED_THREADS - 1) / RED_THREADS,
                                        (long long)(H->partial_n / 2)));
   blocks = std::max(blocks, 1);
@@ -650,11 +757,16 @@ int reduce_t(sp_handle* H, int inst, int field, double* mass, double* energy) {
 extern "C" {
 
 int sp_create(const sp_desc* desc, sp_handle** out) {
+  return sp_create_ensemble(desc, nullptr, 0, out);
+}
+
+int sp_create_ensemble(const sp_desc* desc, const sp_member* members, int count,
+                       sp_handle** out) {
   g_create_error.clear();
   if (!out) return SP_EINVAL;
   *out = nullptr;
   sp_handle* H = new sp_handle();
-  int rc = create(desc, H);
+  int rc = create(desc, members, count, H);
   if (rc != SP_OK) {
     g_create_error = H->err;
     release(H);
@@ -678,17 +790,18 @@ int sp_upload_device(sp_handle* h, int inst, int field, const void* dev, size_t 
 
 int sp_fill_uniform(sp_handle* H, int inst, int field, uint64_t seed, double lo, double hi) {
   if (!H) return SP_EINVAL;
-  const size_t bytes = size_t(H->n[0]) * H->n[1] * (H->dim == 3 ? H->n[2] : 1) * H->esz;
-  if (int rc = check_field(H, inst, field, bytes)) return rc;
+  if (inst < 0 || inst >= H->batch) return fail(H, SP_EINVAL, "instance index out of range");
+  if (int rc = check_field(H, inst, field, size_t(H->geo[inst].sites()) * H->esz)) return rc;
+  const InstGeo& g = H->geo[inst];
   char* base = field_base(H, H->cur, inst, field);
   if (H->esz == 4)
     sp::k_seed<float><<<H->sms * 4, 256, 0, H->stream>>>(
-        reinterpret_cast<float*>(base), H->dim, H->n[0], H->n[1], H->n[2], H->h[0], H->h[1],
-        H->h[2], H->pitch, H->plane, seed, lo, hi);
+        reinterpret_cast<float*>(base), H->dim, g.n[0], g.n[1], g.n[2], H->h[0], H->h[1],
+        H->h[2], g.pitch, g.plane, seed, lo, hi);
   else
     sp::k_seed<double><<<H->sms * 4, 256, 0, H->stream>>>(
-        reinterpret_cast<double*>(base), H->dim, H->n[0], H->n[1], H->n[2], H->h[0], H->h[1],
-        H->h[2], H->pitch, H->plane, seed, lo, hi);
+        reinterpret_cast<double*>(base), H->dim, g.n[0], g.n[1], g.n[2], H->h[0], H->h[1],
+        H->h[2], g.pitch, g.plane, seed, lo, hi);
   SP_CUDA(H, cudaGetLastError());
   return refresh_halos(H, inst, field);
 }
@@ -789,8 +902,10 @@ int sp_autotune(sp_handle* H, int reps) {
   H->launches = launches;
   if (rc) return rc;
   if ((rc = configure(H, best))) return rc;
-  std::lock_guard<std::mutex> lk(g_tune_mutex);
-  g_tuned[tune_key(H)] = best;
+  if (!H->ensemble) {
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    g_tuned[tune_key(H)] = best;
+  }
   return check_err_flag(H);
 }
 
@@ -810,7 +925,9 @@ int sp_kernel_info(const sp_handle* H, int info[8]) {
 int sp_set_dt(sp_handle* H, double dt) {
   if (!H) return SP_EINVAL;
   if (!std::isfinite(dt)) return fail(H, SP_EINVAL, "dt must be finite");
+  if (H->ensemble) return fail(H, SP_EINVAL, "the members of an ensemble keep their own dt");
   if (dt == H->d.dt) return SP_OK;
+  for (InstGeo& g : H->geo) g.dt = dt;
   SP_CUDA(H, cudaStreamSynchronize(H->stream));
   H->d.dt = dt;
   for (int k = 0; k < 2; ++k)
@@ -859,8 +976,8 @@ int sp_field_geometry(const sp_handle* H, int inst, int field, void** dev_origin
   if (inst < 0 || inst >= H->batch || field < 0 || field >= H->nf)
     return fail(M, SP_EINVAL, "instance or field index out of range");
   if (dev_origin) *dev_origin = field_origin(M, H->cur, inst, field);
-  if (pitch) *pitch = H->pitch;
-  if (plane) *plane = H->plane;
+  if (pitch) *pitch = H->geo[inst].pitch;
+  if (plane) *plane = H->geo[inst].plane;
   if (halo)
     for (int a = 0; a < 3; ++a) halo[a] = H->h[a];
   return SP_OK;

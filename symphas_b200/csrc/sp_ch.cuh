@@ -392,7 +392,10 @@ __global__ void __launch_bounds__(TC::NT)
     else
       ok = body(std::integral_constant<int, 2>{}, zi);
     if (!ok) {
-      if (tid == 0) atomicExch(p.err, KERR_TMA_TIMEOUT);
+      if (tid == 0) {
+        atomicExch(p.err, KERR_TMA_TIMEOUT);
+        tma::drain(bars, NSLOT, zi == zi0 ? 0 : zi + R - (zb - R), min(qn, nplanes - 1));
+      }
       return;
     }
     phase = phase == 2 ? 0 : phase + 1;

@@ -51,7 +51,7 @@
 
 namespace sp {
 void register_exact_kernels() {
-  // the BASELINE point sets and SymPhas's defaults (Stencil2d2h<> = <9,6,13>,
+  // the benchmarked point sets <5,6,13> / <7,10,25> and SymPhas's defaults (Stencil2d2h<> = <9,6,13>,
   // Stencil3d2h<> = <15,10,25>, sol/inc/stencilincludes.h:758-792, 884-921)
   SP_EXACT_SET(double, 1, 5, 6, 13, 7, 10, 25)
   SP_EXACT_SET(double, 1, 9, 6, 13, 15, 10, 25)

@@ -410,7 +410,10 @@ __global__ void __launch_bounds__(TC::NT)
 
     // the one barrier of the iteration: planes waited for, stages written
     if (__syncthreads_or(bad)) {
-      if (tid == 0) atomicExch(p.err, KERR_TMA_TIMEOUT);
+      if (tid == 0) {
+        atomicExch(p.err, KERR_TMA_TIMEOUT);
+        tma::drain(bars, NSLOT, zi == zi0 ? 0 : qw, min(qn, nplanes - 1));
+      }
       return;
     }
 
@@ -749,7 +752,14 @@ __global__ void __launch_bounds__(TC::NT)
       }
     }
     if (__syncthreads_or(bad)) {
-      if (tid == 0) atomicExch(p.err, KERR_TMA_TIMEOUT);
+      if (tid == 0) {
+        atomicExch(p.err, KERR_TMA_TIMEOUT);
+        // tiles it .. it + PD were issued into distinct slots (PD < NQ)
+        for (int j = it; j <= it + PD; ++j) {
+          const volatile int* vj = reinterpret_cast<volatile int*>(&items[j % NQ]);
+          if (vj[0] >= 0) tma::mbar_wait(&bars[j % NQ], (j / NQ) & 1);
+        }
+      }
       return;
     }
     const int x0 = (cur.y % ip.ntx) * TX, y0 = (cur.y / ip.ntx) * TY;

@@ -59,6 +59,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return true;
 }
 
+// Error path of a CTA that gave up on a wait: before it leaves, wait (again
+// bounded) for the loads it still has in flight, so that no copy lands in
+// shared memory after the CTA has exited.  Load number q went to ring slot
+// q % nslot with barrier phase (q / nslot) & 1.
+__device__ __forceinline__ void drain(uint64_t* bars, int nslot, int first, int last) {
+  for (int q = first; q <= last; ++q) mbar_wait(&bars[q % nslot], uint32_t((q / nslot) & 1));
+}
+
 __device__ __forceinline__ void load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x,
                                         int y) {
   asm volatile(

@@ -280,6 +280,108 @@ class model_OP_t(Model):
         super().__init__(dim, solver, params, dtype=dtype)
 
 
+class Ensemble(Model):
+    """Independent 2D systems of differing size, model (model_MAMK_t or
+    model_MBMK_t, or all of one model), coefficients and time step, advanced
+    together: every step is one persistent kernel launch over the tiles of
+    all members.  `members` is a list of dicts with keys dims (x, y),
+    model ("AMK", "BMK", or another model class's name), dt and coeff.
+    Instance i is member i in every per-instance call."""
+
+    _IDS = {"A": C.SP_MODEL_A, "B": C.SP_MODEL_B, "AMK": C.SP_MODEL_AMK,
+            "BMK": C.SP_MODEL_BMK}
+
+    def __init__(self, solver, members, h=1.0, boundary=BoundaryType.PERIODIC,
+                 dtype="f32"):
+        if solver.stencil.dim != 2:
+            raise ValueError("ensembles are two-dimensional")
+        if dtype not in _DTYPES:
+            raise ValueError("dtype must be 'f32' or 'f64'")
+        self.dim = 2
+        self.dtype_code, self.np_dtype = _DTYPES[dtype]
+        params = ProblemParameters(members[0]["dims"], h=h, boundary=boundary)
+        d = C.SpDesc()
+        d.dim = 2
+        d.dtype = self.dtype_code
+        d.form = C.SP_FORM_EXACT if solver.form == "exact" else C.SP_FORM_FUSED
+        d.lap_pts, d.gradlap_pts, d.bilap_pts = solver.stencil.points
+        for i in range(6):
+            d.boundary[i] = params.boundary[i]
+            d.boundary_value[i] = params.boundary_value[i]
+        d.h = float(h)
+        arr = (C.SpMember * len(members))()
+        for i, m in enumerate(members):
+            dims = tuple(int(x) for x in m["dims"])
+            if len(dims) != 2:
+                raise ValueError("member %d: two extents (x, y) expected" % i)
+            arr[i].n[0], arr[i].n[1], arr[i].n[2] = dims[0], dims[1], 1
+            arr[i].model = self._IDS[m["model"]]
+            arr[i].dt = float(m["dt"])
+            cs = list(m.get("coeff", ())) + [1.0] * (8 - len(m.get("coeff", ())))
+            for c in range(8):
+                arr[i].coeff[c] = float(cs[c])
+        self.desc = d
+        self.members = [dict(m) for m in members]
+        self.member_dims = [tuple(int(x) for x in m["dims"]) for m in members]
+        self.batch = len(members)
+        self._h = C._H()
+        C.check(C.lib().sp_create_ensemble(ctypes.byref(d), arr, len(members),
+                                           ctypes.byref(self._h)))
+        self.index = 0
+        self.time = None  # members advance by their own dt
+        self.dt = None
+
+    def _shape(self, inst):
+        return tuple(reversed(self.member_dims[inst]))
+
+    def sites(self):
+        return sum(int(np.prod(x)) for x in self.member_dims)
+
+    def set_field(self, field, values, inst=0):
+        a = np.ascontiguousarray(values, dtype=self.np_dtype)
+        if a.shape != self._shape(inst):
+            raise ValueError("field shape %s != %s" % (a.shape, self._shape(inst)))
+        C.check(C.lib().sp_upload(self._h, inst, field, a.ctypes.data, a.nbytes), self._h)
+
+    def get_field(self, field=0, inst=0):
+        out = np.empty(self._shape(inst), dtype=self.np_dtype)
+        C.check(C.lib().sp_download(self._h, inst, field, out.ctypes.data, out.nbytes), self._h)
+        return out
+
+    def eval_rhs(self, field=0, inst=0):
+        out = np.empty(self._shape(inst), dtype=self.np_dtype)
+        C.check(C.lib().sp_eval_rhs(self._h, inst, field, out.ctypes.data, out.nbytes), self._h)
+        return out
+
+    def step(self, n=1):
+        """Advance every member by n steps of its own dt."""
+        C.check(C.lib().sp_step(self._h, int(n)), self._h)
+        self.index += n
+
+    def step_mass(self, *a, **k):
+        raise NotImplementedError("use reduce(inst=i) on ensembles")
+
+
+def ensemble_members(count, seed=0, sides=(64, 96, 128, 256, 384, 512, 768, 1024), h=1.0,
+                     safety=0.4):
+    """A sweep of `count` 2D members: square sides drawn from `sides`, the first
+    half model_MAMK_t and the second half model_MBMK_t, M and kappa drawn from
+    U[0.5, 2], and dt = safety x the forward-Euler stability limit of each
+    member with the 5-point Laplacian (largest eigenvalue 8 / h^2):
+    AMK  2 / (M (8 kappa / h^2 + 2)),  BMK  2 / (M (64 kappa / h^4 + 16 / h^2))."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.choice(sides))
+        M, kappa = (float(v) for v in rng.uniform(0.5, 2.0, 2))
+        if i < count // 2:
+            model, lim = "AMK", 2.0 / (M * (8.0 * kappa / h ** 2 + 2.0))
+        else:
+            model, lim = "BMK", 2.0 / (M * (64.0 * kappa / h ** 4 + 16.0 / h ** 2))
+        out.append({"dims": (n, n), "model": model, "dt": safety * lim, "coeff": (M, kappa)})
+    return out
+
+
 def find_solution(model, dt, steps):
     """symphas::find_solution(model, dt, steps): advance `steps` iterations."""
     model.update(model.time)

@@ -42,3 +42,43 @@ def test_create_rejects_bad_description_without_gpu_work():
     rc = sp.lib().sp_create(ctypes.byref(d), ctypes.byref(h))
     assert rc == _capi.SP_EINVAL
     assert b"dim" in sp.lib().sp_create_error()
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """sizeof and field offsets of sp_desc and sp_member as a C compiler lays
+    them out from the header, against the ctypes mirrors."""
+    import subprocess
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "symphas_b200.h"\n'
+        "int main(void) {\n"
+        '  printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(sp_desc), offsetof(sp_desc, h),\n'
+        "         offsetof(sp_desc, batch), sizeof(sp_member), offsetof(sp_member, dt),\n"
+        "         offsetof(sp_member, coeff));\n"
+        "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    D, M = _capi.SpDesc, _capi.SpMember
+    assert got == [ctypes.sizeof(D), D.h.offset, D.batch.offset, ctypes.sizeof(M), M.dt.offset,
+                   M.coeff.offset]
+
+
+def test_ensemble_rejects_bad_members_without_gpu_work():
+    d = _capi.SpDesc()
+    d.dim = 2
+    mem = (_capi.SpMember * 2)()
+    for i, model in enumerate((_capi.SP_MODEL_A, _capi.SP_MODEL_B)):
+        mem[i].n[0] = mem[i].n[1] = 32
+        mem[i].model = model
+    h = _capi._H()
+    assert sp.lib().sp_create_ensemble(ctypes.byref(d), mem, 2, ctypes.byref(h)) == _capi.SP_EINVAL
+    assert b"AMK" in sp.lib().sp_create_error()
+    d.dim = 3
+    assert sp.lib().sp_create_ensemble(ctypes.byref(d), mem, 2, ctypes.byref(h)) == _capi.SP_EINVAL
+    assert b"two-dimensional" in sp.lib().sp_create_error()
+    d.dim = 2
+    mem[1].n[0] = 2
+    assert sp.lib().sp_create_ensemble(ctypes.byref(d), mem, 2, ctypes.byref(h)) == _capi.SP_EINVAL
