@@ -1,18 +1,34 @@
-"""Headline benchmark: one fused forward-Euler step of Cahn-Hilliard (model B)
-on a 256^3 periodic grid, dx = 1, dt = 0.005, Stencil3d2h<7,10,25>, FP32
-(the bulk path), seeded uniform noise +-0.1 around psi_bar = -0.2.
+"""Throughput of the fused forward-Euler finite-difference step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload b3d|ensemble|c3d]
 
-A timed step is one fused-step launch; a 256 MiB buffer is written before
-every timed step so the L2 (126 MB) holds none of the field, and each step is
-timed with CUDA events on the solver's stream.  With N > 1 (torchrun), every
-rank advances its own replica (the path runs on one GPU; replicas only) and
-the job time is the maximum over ranks.  Prints one JSON line (rank 0).
+Workloads (synthetic seeded fields; site-updates/s counts interior sites
+advanced by one step, summed over instances):
+
+  b3d       (default, the headline) Cahn-Hilliard (model B) on a 256^3
+            periodic grid, dx 1, dt 0.005, Stencil3d2h<7,10,25>, FP32 fused
+            step, psi_bar -0.2 +- 0.1.  A 256 MiB buffer is written before
+            every timed step so the L2 (126 MB) holds none of the field; each
+            step is timed with CUDA events on the solver's stream.
+  ensemble  1024 independent 2D members, sides drawn from {64, 96, 128, 256,
+            384, 512, 768, 1024}, first half model A (AMK: M, kappa), second
+            half model B (BMK), M and kappa from U[0.5, 2], dt = 40% of each
+            member's stability limit, +-0.1 noise, FP32 fused, periodic; one
+            persistent launch per step, steps replayed from CUDA graphs.  The
+            fields (~2.2 GB per buffer) exceed the L2, the K steps are timed
+            as one region.
+  c3d       model C (psi conserved, eta not, gamma 0.5), 8 instances of 256^3
+            periodic, dx 1, dt 0.005, FP32 fused, psi_bar 0.1 +- 0.1 and eta
+            +-0.1; one launch advances all 8 (2.1 GB per buffer, beyond L2).
+
+With N > 1 (torchrun), every rank advances its own replica (the path runs on
+one GPU; replicas only) and the job time is the maximum over ranks.  Prints
+one JSON line (rank 0).
 
 --impl reference times the CPU implementation of the same path (the C
 restatement of SymPhas's SolverFT in oracle/, FP64 as SymPhas computes, all
-host threads) on the same grid: one step per timed step.
+host threads) on the same workload: a bounded sample per timed step.
 """
 import argparse
 import json
@@ -28,15 +44,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "site-updates/s + %HBM roofline; time-to-t_end surrogate vs plain FD at ≤1% L2"
 UNIT = "site-updates/s"
-N_GRID = 256
-DT = 0.005
-WORKLOAD = ("Cahn-Hilliard (model B) 3D 256^3 periodic, dx 1, dt 0.005, "
-            "Stencil3d2h<7,10,25>, fused step, psi_bar -0.2 +- 0.1 seeded noise")
-ALG_BYTES_PER_SITE = 8  # one FP32 read and one FP32 write of the field per step
 CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_fd3d_modelB_256cube_f32.json")
 
 
 def parse():
@@ -45,6 +55,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="b3d", choices=["b3d", "ensemble", "c3d"])
     ap.add_argument("--e2e-inner", type=int, default=100,
                     help="FD steps per end-to-end call (upload, steps, download)")
     return ap.parse_args()
@@ -103,56 +114,197 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def cpu_port_rate(seconds, threads):
-    """Site-updates/s of the CPU restatement (oracle) on the same grid, FP64."""
+def oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
     import spo
 
-    n = N_GRID
-    d = spo.make_desc(3, (n, n, n), spo.MODEL_B, 1.0, DT)
-    x = spo.seed_uniform(20261203, -0.3, -0.1, n ** 3).reshape(n, n, n)
-    sysm = spo.System(d, x, threads)
-    sysm.step(1)  # warm-up
+    return spo
+
+
+class B3D:
+    """Model B 3D 256^3 FP32 (the headline)."""
+
+    name = "b3d"
+    n = 256
+    dt = 0.005
+    dtype = "f32"
+    bytes_per_site = 8  # one FP32 read and one FP32 write of the field per step
+    flush_each_step = True
+    kernel = "fused model B step (k_fd3d / k_ch3d, the autotuned tile variant)"
+    traffic_file = os.path.join(ROOT, "profiles", "k_fd3d_modelB_256cube_f32.json")
+    workload = ("Cahn-Hilliard (model B) 3D 256^3 periodic, dx 1, dt 0.005, "
+                "Stencil3d2h<7,10,25>, fused step, psi_bar -0.2 +- 0.1 seeded noise")
+
+    def __init__(self, sp, rank, stream):
+        n = self.n
+        self.sites = float(n) ** 3
+        self.model = sp.model_MB_t(3, sp.SolverFT(sp.Stencil3d2h(7, 10, 25), form="fused"),
+                                   sp.ProblemParameters((n, n, n), h=1.0), dtype="f32")
+        self.model.set_stream(stream.cuda_stream)
+        self.model.fill_uniform(0, 20261203 + rank, -0.3, -0.1)
+        self.shape = self.model.autotune(20)  # setup, not timed
+        self.fields = [(0, 0, int(self.sites))]  # (instance, field, sites)
+
+    def step(self, k):
+        self.model.step(self.dt, k)
+
+    def config(self):
+        return {"grid": [self.n] * 3, "kernel_shape": self.shape}
+
+    @classmethod
+    def cpu_system(cls, threads):
+        spo = oracle()
+        n = cls.n
+        d = spo.make_desc(3, (n, n, n), spo.MODEL_B, 1.0, cls.dt)
+        x = spo.seed_uniform(20261203, -0.3, -0.1, n ** 3).reshape(n, n, n)
+        sysm = spo.System(d, x, threads)
+        return (lambda: sysm.step(1)), float(n) ** 3, sysm.close, (
+            "SolverFT steps of model B 256^3 FP64 (C restatement, %d threads)" % threads)
+
+
+class C3D(B3D):
+    """Model C, 8 instances of 256^3, FP32."""
+
+    name = "c3d"
+    batch = 8
+    bytes_per_site = 16  # two fields, each read and written once per step
+    flush_each_step = False
+    kernel = "fused model C step (k_fd3d, two fields, the autotuned tile variant)"
+    traffic_file = os.path.join(ROOT, "profiles", "k_fd3d_modelC_8x256cube_f32.json")
+    workload = ("model C (gamma 0.5) 3D, 8 instances of 256^3 periodic, dx 1, dt 0.005, "
+                "Stencil3d2h<7,10,25>, fused step, psi 0.1 +- 0.1, eta +- 0.1 seeded noise")
+
+    def __init__(self, sp, rank, stream):
+        n = self.n
+        self.sites = float(n) ** 3 * self.batch
+        self.model = sp.model_MC_t(3, sp.SolverFT(sp.Stencil3d2h(7, 10, 25), form="fused"),
+                                   sp.ProblemParameters((n, n, n), h=1.0), coeff=(0.5,),
+                                   dtype="f32", batch=self.batch)
+        self.model.set_stream(stream.cuda_stream)
+        for i in range(self.batch):
+            self.model.fill_uniform(0, 7000 + 64 * rank + 2 * i, 0.0, 0.2, inst=i)
+            self.model.fill_uniform(1, 7001 + 64 * rank + 2 * i, -0.1, 0.1, inst=i)
+        self.shape = self.model.autotune(5)
+        self.fields = [(i, f, n ** 3) for i in range(self.batch) for f in range(2)]
+
+    def config(self):
+        return {"grid": [self.n] * 3, "instances": self.batch, "kernel_shape": self.shape}
+
+    @classmethod
+    def cpu_system(cls, threads):
+        spo = oracle()
+        import numpy as np
+
+        n = cls.n
+        d = spo.make_desc(3, (n, n, n), spo.MODEL_C, 1.0, cls.dt, coeff=(0.5,))
+        x = np.stack([spo.seed_uniform(7000, 0.0, 0.2, n ** 3),
+                      spo.seed_uniform(7001, -0.1, 0.1, n ** 3)]).reshape(2, n, n, n)
+        sysm = spo.System(d, x, threads)
+        return (lambda: sysm.step(1)), float(n) ** 3, sysm.close, (
+            "SolverFT steps of one model C 256^3 instance FP64 (C restatement, %d threads)"
+            % threads)
+
+
+class Ens:
+    """1024 2D members of uneven sizes, models AMK / BMK, FP32."""
+
+    name = "ensemble"
+    count = 1024
+    seed = 20261203
+    dtype = "f32"
+    bytes_per_site = 8
+    flush_each_step = False
+    kernel = "k_fd2d (persistent tile queue over every member, AMK and BMK right-hand sides)"
+    traffic_file = os.path.join(ROOT, "profiles", "k_fd2d_ensemble1024_f32.json")
+    workload = ("ensemble of 1024 2D periodic members, sides from {64,96,128,256,384,512,768,"
+                "1024}, half model A (AMK) half model B (BMK), M and kappa U[0.5,2], dt 40% of "
+                "each stability limit, Stencil2d2h<5,6,13>, fused step, +-0.1 seeded noise")
+
+    def __init__(self, sp, rank, stream):
+        self.members = sp.ensemble_members(self.count, seed=self.seed)
+        self.model = sp.Ensemble(sp.SolverFT(sp.Stencil2d2h(5, 6, 13), form="fused"),
+                                 self.members, dtype="f32")
+        self.model.set_stream(stream.cuda_stream)
+        for i in range(self.count):
+            self.model.fill_uniform(0, self.seed + 4096 * rank + i, -0.1, 0.1, inst=i)
+        self.sites = float(self.model.sites())
+        self.shape = self.model.autotune(5)
+        self.fields = [(i, 0, int(m["dims"][0] * m["dims"][1]))
+                       for i, m in enumerate(self.members)]
+
+    def step(self, k):
+        self.model.step(k)
+
+    def config(self):
+        sides = sorted({m["dims"][0] for m in self.members})
+        return {"members": self.count, "sides": sides, "sites": int(self.sites),
+                "kernel_shape": self.shape}
+
+    @classmethod
+    def cpu_system(cls, threads):
+        """Every 8th member (128 of them, both models, all sizes), all threads
+        over members (one member per thread, as independent SymPhas models)."""
+        spo = oracle()
+        import numpy as np
+
+        import symphas_b200.model as spm  # the member generator only (host code)
+
+        members = spm.ensemble_members(cls.count, seed=cls.seed)[::8]
+        ids = {"AMK": spo.MODEL_AMK, "BMK": spo.MODEL_BMK}
+        descs = [spo.make_desc(2, m["dims"], ids[m["model"]], 1.0, m["dt"], coeff=m["coeff"])
+                 for m in members]
+        fields = [spo.seed_uniform(cls.seed + i, -0.1, 0.1, m["dims"][0] * m["dims"][1])
+                  for i, m in enumerate(members)]
+        sites = float(sum(m["dims"][0] * m["dims"][1] for m in members))
+
+        def one():
+            spo.run_batch(descs, fields, [1] * len(descs), threads)
+
+        return one, sites, (lambda: None), (
+            "one SolverFT step of 128 of the 1024 members (every 8th) FP64 "
+            "(C restatement, %d threads over members)" % threads)
+
+
+WORKLOADS = {"b3d": B3D, "c3d": C3D, "ensemble": Ens}
+
+
+def cpu_rate(W, seconds, threads):
+    """Site-updates/s of the CPU restatement (oracle) on the workload, FP64."""
+    step, sites, close, what = W.cpu_system(threads)
+    step()  # warm-up
     steps, t0 = 0, time.perf_counter()
     while True:
-        sysm.step(1)
+        step()
         steps += 1
         el = time.perf_counter() - t0
         if el >= seconds and steps >= 2:
             break
-    sysm.close()
-    return steps * float(n ** 3) / el, steps, el, np
+    close()
+    return steps * sites / el, "%d %s, %.1f s" % (steps, what, el)
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import spo
-
+    W = WORKLOADS[args.workload]
     threads = os.cpu_count() or 1
-    n = N_GRID
-    d = spo.make_desc(3, (n, n, n), spo.MODEL_B, 1.0, DT)
-    x = spo.seed_uniform(20261203, -0.3, -0.1, n ** 3).reshape(n, n, n)
-    sysm = spo.System(d, x, threads)
+    step, sites, close, what = W.cpu_system(threads)
     for _ in range(args.warmup):
-        sysm.step(1)
+        step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        sysm.step(1)
+        step()
     el = time.perf_counter() - t0
-    sysm.close()
-    value = args.steps * float(n ** 3) / el
-    sample = "%d SolverFT steps of model B 256^3 FP64 (C restatement, %d threads)" % (
-        args.steps, threads)
+    close()
+    value = args.steps * sites / el
+    sample = "%d %s" % (args.steps, what)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD.replace("fused step", "SolverFT step"), "grid": n},
+        "config": {"workload": W.workload.replace("fused step", "SolverFT step")},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -178,42 +330,50 @@ def run_ours(args):
 
     import symphas_b200 as sp
 
-    n = N_GRID
-    sites = float(n) ** 3
+    W = WORKLOADS[args.workload]
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    model = sp.model_MB_t(3, sp.SolverFT(sp.Stencil3d2h(7, 10, 25), form="fused"),
-                          sp.ProblemParameters((n, n, n), h=1.0), dtype="f32")
-    model.set_stream(stream.cuda_stream)
-    model.fill_uniform(0, 20261203 + rank, -0.3, -0.1)
-    tile = model.autotune(20)  # pick the fastest tile shape (setup, not timed)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB
-
-    for _ in range(max(args.warmup, 3)):
-        flush.zero_()
-        model.step(DT, 1)
+    w = W(sp, rank, stream)
+    sites = w.sites
+    warmup = max(args.warmup, 3)
+    flush = None
+    if W.flush_each_step:
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB
+    for _ in range(warmup):
+        if flush is not None:
+            flush.zero_()
+        w.step(1)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     gpu_index = os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[local]
     clocks = Clocks(gpu_index)
     clocks.start()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    launches0 = model.launch_count()
+    launches0 = w.model.launch_count()
     torch.cuda.synchronize()
-    for e0, e1 in ev:
-        flush.zero_()
+    if flush is not None:
+        # L2 flushed before every step; each step timed on the solver's stream
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        for e0, e1 in ev:
+            flush.zero_()
+            e0.record(stream)
+            w.step(1)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms = sum(a.elapsed_time(b) for a, b in ev)
+    else:
+        # fields larger than the L2: the K steps (graph-replayed) as one region
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        model.step(DT, 1)
+        w.step(args.steps)
         e1.record(stream)
-    torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        total_ms = e0.elapsed_time(e1)
     if dist:
         dist.barrier()
     clk = clocks.stop()
-    launches = model.launch_count() - launches0
-    per = [a.elapsed_time(b) for a, b in ev]
-    total_ms = sum(per)
+    launches = w.model.launch_count() - launches0
     t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -221,25 +381,40 @@ def run_ours(args):
     value = world * args.steps * sites / (job_ms * 1e-3)
     launch_ms = total_ms / args.steps
 
-    # end to end: pinned host field -> upload -> e2e_inner steps -> download
-    nbytes = int(sites) * 4
-    host_in = torch.empty(int(sites), dtype=torch.float32, pin_memory=True)
-    host_out = torch.empty(int(sites), dtype=torch.float32, pin_memory=True)
-    model.download_to(0, host_in.data_ptr(), nbytes)
-    e2e_calls = max(3, args.steps // 40)
+    # end to end through the public API: every field of the step's input from
+    # pinned host memory, e2e_inner steps, every field back to pinned memory
+    esz = 4
+    offs, total = [], 0
+    for inst, f, cnt in w.fields:
+        offs.append(total)
+        total += cnt
+    host_in = torch.empty(total, dtype=torch.float32, pin_memory=True)
+    host_out = torch.empty(total, dtype=torch.float32, pin_memory=True)
+    nbytes = total * esz
+
+    def download(buf):
+        for (inst, f, cnt), o in zip(w.fields, offs):
+            w.model.download_to(f, buf.data_ptr() + o * esz, cnt * esz, inst=inst)
+
+    def upload(buf):
+        for (inst, f, cnt), o in zip(w.fields, offs):
+            w.model.upload_from(f, buf.data_ptr() + o * esz, cnt * esz, inst=inst)
+
+    download(host_in)
+    e2e_calls = 3
     for _ in range(2):
-        model.upload_from(0, host_in.data_ptr(), nbytes)
-        model.step(DT, args.e2e_inner)
-        model.download_to(0, host_out.data_ptr(), nbytes)
+        upload(host_in)
+        w.step(args.e2e_inner)
+        download(host_out)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e_start.record(stream)
     for _ in range(e2e_calls):
-        model.upload_from(0, host_in.data_ptr(), nbytes)
-        model.step(DT, args.e2e_inner)
-        model.download_to(0, host_out.data_ptr(), nbytes)
+        upload(host_in)
+        w.step(args.e2e_inner)
+        download(host_out)
     e_end.record(stream)
     torch.cuda.synchronize()
     t = torch.tensor([e_start.elapsed_time(e_end)], dtype=torch.float64, device="cuda")
@@ -247,7 +422,7 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_ms = float(t.item()) / e2e_calls
     e2e_value = world * args.e2e_inner * sites / (e2e_ms * 1e-3)
-    model.close()
+    w.model.close()
 
     if rank != 0:
         if dist:
@@ -255,45 +430,44 @@ def run_ours(args):
         return 0
 
     peak, peak_kind = measured_peak()
-    achieved = sites * ALG_BYTES_PER_SITE / (launch_ms * 1e-3) / 1e9
+    alg_bytes = sites * W.bytes_per_site
+    achieved = alg_bytes / (launch_ms * 1e-3) / 1e9
     traffic = None
     try:
-        traffic = json.load(open(PROFILE_TRAFFIC))["dram_bytes_per_launch"]
+        traffic = json.load(open(W.traffic_file))["dram_bytes_per_launch"]
     except Exception:
         pass
+    cfg = {"workload": W.workload, "global_batch": world,
+           "l2": ("256 MiB buffer written before every timed step (L2 flushed)"
+                  if W.flush_each_step else
+                  "fields larger than the 126 MB L2 (%.2f GB read per step)" % (alg_bytes / 2e9)),
+           "parallelism": "replicas" if world > 1 else "single GPU"}
+    cfg.update(w.config())
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": max(args.warmup, 3), "ms_per_step": job_ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": [n, n, n], "global_batch": world,
-                   "l2": "256 MiB buffer written before every timed step (L2 flushed)",
-                   "parallelism": "replicas" if world > 1 else "single GPU",
-                   "kernel_shape": tile},
+        "warmup": warmup, "ms_per_step": job_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": W.dtype,
+        "data": "synthetic", "config": cfg,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "peak_kind": peak_kind, "kernel": "k_fd3d (fused model B step)",
-                     "alg_bytes_per_launch": sites * ALG_BYTES_PER_SITE},
+                     "peak_kind": peak_kind, "kernel": W.kernel,
+                     "alg_bytes_per_launch": alg_bytes},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": nbytes,
-                "step": "upload field from pinned host, %d fused steps, download field" %
-                        args.e2e_inner},
+                "step": "upload every field from pinned host, %d fused steps, download every "
+                        "field" % args.e2e_inner},
         "gpu_launches": launches,
         "clocks": clk,
     }
     if world == 1:
         threads = os.cpu_count() or 1
-        rate, steps, el, _ = cpu_port_rate(10.0, threads)
-        line["cpu_baseline"] = {
-            "value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "%d SolverFT steps of model B 256^3 FP64 (C restatement), %.1f s" % (
-                steps, el)}
+        rate, sample = cpu_rate(W, 10.0, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": sample}
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
     return 0
-
-
 def main():
     args = parse()
     if args.impl == "reference":

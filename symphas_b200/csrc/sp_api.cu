@@ -289,7 +289,10 @@ int fill_halo_t(sp_handle* H, int which, int inst, int f) {
     p.bc[s] = H->d.boundary[s];
     p.bv[s] = T(H->d.boundary_value[s]);
   }
-  sp::k_fill_halo<T><<<H->sms * 4, 256, 0, H->stream>>>(p);
+  const long long cells = (g.n[0] + 2LL * H->h[0]) * (g.n[1] + 2LL * H->h[1]) *
+                          (H->dim == 3 ? g.n[2] + 2LL * H->h[2] : 1);
+  const int blocks = int(std::min<long long>(H->sms * 4LL, (cells + 255) / 256));
+  sp::k_fill_halo<T><<<blocks, 256, 0, H->stream>>>(p);
   SP_CUDA(H, cudaGetLastError());
   return SP_OK;
 }

@@ -218,15 +218,19 @@ __global__ void __launch_bounds__(TC::NT)
   T* orow[SPT];
   bool rowin[SPT];
   long long yo[SPT];
-  bool simple = vec_ok && xo == 0;
 #pragma unroll
   for (int k = 0; k < SPT; ++k) {
     const int y = y0 + row0 + k;
     rowin[k] = xin && y < p.n[1];
     yo[k] = image_offset(p.per[1], y, 1, p.n[1], R, p.pitch);
-    simple = simple && rowin[k] && yo[k] == 0;
     orow[k] = p.out[blockIdx.z] + (long long)(y + p.h[1]) * p.pitch + (x + p.h[0]);
   }
+  // the whole tile inside the domain, away from every periodic face, in whole
+  // vectors: straight-line stores (the same for every thread of the block)
+  const bool plain = (p.n[0] % W == 0) && x0 + TX <= p.n[0] && y0 + TY <= p.n[1] &&
+                     (!p.per[0] || (x0 >= R && x0 + TX <= p.n[0] - R)) &&
+                     (!p.per[1] || (y0 >= R && y0 + TY <= p.n[1] - R));
+  const bool ragged = xin && !vec_ok;
   const bool do_mass = p.partial != nullptr;
   // the mu cell beyond this thread's own ones, if any: own cells are stage
   // rows RS..TY+RS-1 and column groups RSA/W..RSA/W+TXT-1; the ring is the
@@ -356,16 +360,14 @@ __global__ void __launch_bounds__(TC::NT)
         if constexpr (RH::has_m) r = mob * r;
         nv[k] = p.rhs_only ? r : fmadd<true>(vdt, r, qpsi[IM][k]);
       }
-      if (simple && zo == 0) {
+      if (plain && zo == 0) {
 #pragma unroll
         for (int k = 0; k < SPT; ++k) *reinterpret_cast<V*>(orow[k] + zoff) = nv[k];
       } else {
 #pragma unroll
         for (int k = 0; k < SPT; ++k) {
-          if (!rowin[k]) continue;
-          if (vec_ok)
-            put_images(orow[k] + zoff, nv[k], xo, yo[k], zo);
-          else
+          put_images_pred(orow[k] + zoff, nv[k], rowin[k] && vec_ok, xo, yo[k], zo);
+          if (ragged && rowin[k])
             store_group<T, W, 3, R>(p.out[blockIdx.z], x, y0 + row0 + k, zi, nv[k], p.n, p.h,
                                     p.per, p.pitch, p.plane);
         }

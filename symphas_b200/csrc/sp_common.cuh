@@ -150,9 +150,11 @@ __device__ __forceinline__ vec_t<T, W> load_at(const T* p) {
   }
 }
 
-// Evaluation context of one W-wide site group: shared-memory offsets of the
-// field planes (NZ planes centred at ZR) and staged-operand planes, relative
-// to `base`; PW and SW are the row pitches of the field and stage tiles.
+// Evaluation context of one W-wide site group: shared-memory pointers to the
+// group's site in the field planes (NZ planes centred at ZR) and in the
+// staged-operand planes; PW and SW are the row pitches of the field and stage
+// tiles.  Holding pointers (not offsets from a base) makes every stencil
+// point a compile-time displacement of one of them, i.e. a load immediate.
 template <class T, int W, bool CONTRACT, int DIM, int LP, int GP, int BP, int NF, int NZ, int ZR,
           int PW, int NS, int NSZ, int SZR, int SW>
 struct Ctx {
@@ -160,9 +162,8 @@ struct Ctx {
   using value_type = vec_t<T, W>;
   static constexpr bool contract = CONTRACT;  // a*b + c may round once
   static constexpr int dim = DIM, lap_points = LP, gradlap_points = GP, bilap_points = BP;
-  const T* base;
-  int fo[NF][NZ];
-  int so[NS > 0 ? NS : 1][NSZ > 0 ? NSZ : 1];
+  const T* fo[NF][NZ];
+  const T* so[NS > 0 ? NS : 1][NSZ > 0 ? NSZ : 1];
   value_type divh2, divh3, divh4;
   const T* cf;
   template <int I, int X, int Y, int Z>
@@ -170,13 +171,13 @@ struct Ctx {
     static_assert(I >= 1 && I <= NF, "field index");
     static_assert(Z + ZR >= 0 && Z + ZR < NZ, "z reach beyond the loaded planes");
     static_assert(DIM == 3 || Z == 0, "z offset in 2D");
-    return load_at<T, W, X>(base + fo[I - 1][Z + ZR] + Y * PW);
+    return load_at<T, W, X>(fo[I - 1][Z + ZR] + Y * PW);
   }
   template <int K, int X, int Y, int Z>
   __device__ __forceinline__ value_type stg() const {
     static_assert(K >= 0 && K < NS, "stage index");
     static_assert(Z + SZR >= 0 && Z + SZR < NSZ, "z reach beyond the staged planes");
-    return load_at<T, W, X>(base + so[K][Z + SZR] + Y * SW);
+    return load_at<T, W, X>(so[K][Z + SZR] + Y * SW);
   }
   __device__ __forceinline__ value_type coef(int i) const { return value_type(cf[i - 1]); }
 };

@@ -353,6 +353,41 @@ struct Ev<Pow<N, A>> {
     return rpow<N>(Ev<A>::template at<X, Y, Z>(e.a, c));
   }
 };
+template <class A>
+struct IsLeaf {
+  static constexpr bool value = false;
+};
+template <int I>
+struct IsLeaf<Var<I>> {
+  static constexpr bool value = true;
+};
+template <int K>
+struct IsLeaf<StageRef<K>> {
+  static constexpr bool value = true;
+};
+
+// (value at x-1) + (value at x+1) at every lane of a W-group shifted by X.
+// For a field or staged operand the lanes are summed one by one from the
+// aligned groups at X-W, X and X+W (scalar adds, rounded as the vector add
+// would round each lane), so no register shuffles build the shifted groups.
+template <int X, int Y, int Z, class A, class C>
+__device__ __forceinline__ typename C::value_type xpair(const A& a, const C& c) {
+  using V = typename C::value_type;
+  constexpr int W = int(sizeof(V) / sizeof(typename C::scalar_type));
+  if constexpr (IsLeaf<A>::value && W > 1 && X % W == 0) {
+    const V lo = Ev<A>::template at<X - W, Y, Z>(a, c);
+    const V mid = Ev<A>::template at<X, Y, Z>(a, c);
+    const V hi = Ev<A>::template at<X + W, Y, Z>(a, c);
+    V r;
+#pragma unroll
+    for (int j = 0; j < W; ++j)
+      r.v[j] = ((j == 0) ? lo.v[W - 1] : mid.v[j - 1]) + ((j == W - 1) ? hi.v[0] : mid.v[j + 1]);
+    return r;
+  } else {
+    return Ev<A>::template at<X - 1, Y, Z>(a, c) + Ev<A>::template at<X + 1, Y, Z>(a, c);
+  }
+}
+
 // Laplacian in a context that may contract and reassociate (the fused form):
 // the 5- and 7-point sums become a balanced tree ending in one FMA, which
 // shortens the dependency chain; other point sets, and the exact form, keep
@@ -364,11 +399,11 @@ struct Ev<Lap<A>> {
     using T = typename C::value_type;
     Shifted<A, X, Y, Z, C> s{e.a, c};
     if constexpr (C::contract && C::dim == 2 && C::lap_points == 5) {
-      const T sx = s.template at<-1, 0, 0>() + s.template at<1, 0, 0>();
+      const T sx = xpair<X, Y, Z>(e.a, c);
       const T sy = s.template at<0, -1, 0>() + s.template at<0, 1, 0>();
       return fmadd<true>(T(-4.0) * c.divh2, s.template at<0, 0, 0>(), (sx + sy) * c.divh2);
     } else if constexpr (C::contract && C::dim == 3 && C::lap_points == 7) {
-      const T sx = s.template at<-1, 0, 0>() + s.template at<1, 0, 0>();
+      const T sx = xpair<X, Y, Z>(e.a, c);
       const T sy = s.template at<0, -1, 0>() + s.template at<0, 1, 0>();
       const T sz = s.template at<0, 0, -1>() + s.template at<0, 0, 1>();
       return fmadd<true>(T(-6.0) * c.divh2, s.template at<0, 0, 0>(), ((sx + sy) + sz) * c.divh2);

@@ -177,24 +177,45 @@ __device__ __forceinline__ long long image_offset(int per, int c, int w, int n, 
   return 0;
 }
 
-// one vector store and its periodic images (x, y, z and their combinations);
-// the image offsets are 0 where there is no image
-template <class V, class T>
-__device__ __forceinline__ void put_images(T* p, const V& v, long long xo, long long yo,
-                                           long long zo) {
-  *reinterpret_cast<V*>(p) = v;
-  if (xo) *reinterpret_cast<V*>(p + xo) = v;
-  if (yo) {
-    *reinterpret_cast<V*>(p + yo) = v;
-    if (xo) *reinterpret_cast<V*>(p + yo + xo) = v;
-  }
-  if (zo) {
-    *reinterpret_cast<V*>(p + zo) = v;
-    if (xo) *reinterpret_cast<V*>(p + zo + xo) = v;
-    if (yo) {
-      *reinterpret_cast<V*>(p + zo + yo) = v;
-      if (xo) *reinterpret_cast<V*>(p + zo + yo + xo) = v;
-    }
+// Vector store of v at p when `on`, as one predicated instruction.  Periodic
+// images belong to the lanes at a face, and those lanes sit in every warp of
+// a face tile: a branch around their stores would diverge every such warp,
+// a predicated store costs each warp one issue slot.  p need only be a valid
+// address when `on`.
+__device__ __forceinline__ void st_if(float* p, const Vec<float, 2>& v, bool on) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %3, 0;\n\t"
+      "@q st.global.v2.f32 [%0], {%1, %2};\n\t}" ::"l"(p),
+      "f"(v.v[0]), "f"(v.v[1]), "r"(int(on))
+      : "memory");
+}
+__device__ __forceinline__ void st_if(double* p, const Vec<double, 2>& v, bool on) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %3, 0;\n\t"
+      "@q st.global.v2.f64 [%0], {%1, %2};\n\t}" ::"l"(p),
+      "d"(v.v[0]), "d"(v.v[1]), "r"(int(on))
+      : "memory");
+}
+template <class T, class V>
+__device__ __forceinline__ void st_if(T* p, const V& v, bool on) {
+  if (on) *reinterpret_cast<V*>(p) = v;
+}
+
+// A whole W-group at b (padded address of an interior site) and its periodic
+// images (offsets xo, yo, zo; 0 where there is none), all predicated; `in`
+// says whether the group exists.  zo is uniform across the block (one plane).
+template <class T, class V>
+__device__ __forceinline__ void put_images_pred(T* b, const V& v, bool in, long long xo,
+                                                long long yo, long long zo) {
+  st_if(b, v, in);
+  st_if(b + xo, v, in && xo != 0);
+  st_if(b + yo, v, in && yo != 0);
+  st_if(b + xo + yo, v, in && xo != 0 && yo != 0);
+  if (zo != 0) {
+    st_if(b + zo, v, in);
+    st_if(b + zo + xo, v, in && xo != 0);
+    st_if(b + zo + yo, v, in && yo != 0);
+    st_if(b + zo + xo + yo, v, in && xo != 0 && yo != 0);
   }
 }
 
@@ -246,6 +267,7 @@ struct Fd3 {
   static constexpr int SWC = SW / W;        // column groups of a stage row
   static constexpr int XC = 2 * RSA / W;    // extra column groups left and right
   static constexpr int NE = 2 * RS * SWC + TY * XC;  // stage cells beyond one per row group
+  static constexpr int NX = (NE + NT - 1) / NT;       // of them, per thread at most
   static constexpr size_t SMEM =
       256 + sizeof(T) * (size_t(NF) * NSLOT * PLANE + size_t(NS) * NSR * SPL);
   static_assert(U == R, "the newest plane needed is R ahead");
@@ -253,8 +275,33 @@ struct Fd3 {
   static_assert(NSLOT <= 32, "barrier header holds 32 slots");
   static_assert(PW <= 256 && PH <= 256, "TMA box limit");
   static_assert((PW * sizeof(T)) % 16 == 0, "TMA box rows must be whole 16-byte units");
-  static_assert(NE <= NT, "one extra stage cell per thread at most");
+  static_assert(NX <= 4, "extra stage cells per thread");
 };
+
+// the stage cells of a tile beyond the row groups of its threads: the RS rows
+// below the tile (all column groups), then the XC column groups right of each
+// row; thread tid takes cells tid, tid + NT, ... (row -1 marks none)
+template <int NE, int NT, int NX, int TY, int RS, int SWC, int XC, int TXT>
+__device__ __forceinline__ void extra_cells(int tid, int (&xsr)[NX > 0 ? NX : 1],
+                                            int (&xsc)[NX > 0 ? NX : 1]) {
+#pragma unroll
+  for (int j = 0; j < (NX > 0 ? NX : 1); ++j) {
+    const int e = tid + j * NT;
+    xsr[j] = -1;
+    xsc[j] = 0;
+    if constexpr (NE > 0) {
+      if (e >= NE) continue;
+      if (e < 2 * RS * SWC) {
+        xsr[j] = TY + e / SWC;
+        xsc[j] = e % SWC;
+      } else {
+        const int e2 = e - 2 * RS * SWC;
+        xsr[j] = e2 / XC;
+        xsc[j] = TXT + e2 % XC;
+      }
+    }
+  }
+}
 
 template <class M, class T, int LP, int GP, int BP, class TC, bool EXACT>
 __global__ void __launch_bounds__(TC::NT)
@@ -264,7 +311,8 @@ __global__ void __launch_bounds__(TC::NT)
                 NF = K::NF, NS = K::NS, R = K::R, RS = K::RS, RSA = K::RSA, HXA = K::HXA,
                 PW = K::PW, PH = K::PH, PLANE = K::PLANE, NSLOT = K::NSLOT, SW = K::SW,
                 SPL = K::SPL, NSR = K::NSR, NT = K::NT, RD = K::RD, RI = K::RI, U = K::U,
-                WARM = K::WARM, SWC = K::SWC, XC = K::XC, NE = K::NE;
+                WARM = K::WARM, SWC = K::SWC, XC = K::XC, NE = K::NE, NX = K::NX, L = K::L;
+  constexpr int NX1 = NX > 0 ? NX : 1;
   constexpr uint32_t TXB = uint32_t(NF * PW * PH * sizeof(T));
   using V = vec_t<T, W>;
   constexpr int SO = NS > 1 ? 2 : 1;
@@ -299,34 +347,26 @@ __global__ void __launch_bounds__(TC::NT)
   T* orow[SPT][NF];
   bool rowin[SPT];
   long long yo[SPT];
-  // `simple`: every row of this thread is inside, stores whole vectors and has
-  // no x or y image -- its stores are then straight-line code
-  bool simple = vec_ok && xo == 0;
 #pragma unroll
   for (int k = 0; k < SPT; ++k) {
     const int y = y0 + row0 + k;
     rowin[k] = xin && y < p.n[1];
     yo[k] = image_offset(p.per[1], y, 1, p.n[1], R, p.pitch);
-    simple = simple && rowin[k] && yo[k] == 0;
 #pragma unroll
     for (int f = 0; f < NF; ++f)
       orow[k][f] = p.out[inst * NF + f] + (long long)(y + p.h[1]) * p.pitch + (x + p.h[0]);
   }
+  // `plain`: the whole tile lies inside the domain, away from every periodic
+  // face, in whole vectors: its stores are straight-line code.  The same for
+  // every thread of the block.
+  const bool plain = (p.n[0] % W == 0) && x0 + TX <= p.n[0] && y0 + TY <= p.n[1] &&
+                     (!p.per[0] || (x0 >= R && x0 + TX <= p.n[0] - R)) &&
+                     (!p.per[1] || (y0 >= R && y0 + TY <= p.n[1] - R));
+  const bool ragged = xin && !vec_ok;  // a group cut by the end of the row
   const bool do_mass = p.partial != nullptr;
-  // the stage cell beyond this thread's row groups, if any
-  int xsr = -1, xsc = 0;
-  if constexpr (NS > 0) {
-    if (tid < NE) {
-      if (tid < 2 * RS * SWC) {
-        xsr = TY + tid / SWC;
-        xsc = tid % SWC;
-      } else {
-        const int e = tid - 2 * RS * SWC;
-        xsr = e / XC;
-        xsc = TXT + e % XC;
-      }
-    }
-  }
+  // the stage cells beyond this thread's row groups, if any
+  int xsr[NX1], xsc[NX1];
+  extra_cells<NE, NT, NX, TY, RS, SWC, XC, TXT>(tid, xsr, xsc);
 
   if (tid == 0) {
     for (int s = 0; s < NSLOT; ++s) tma::mbar_init(&bars[s], 1);
@@ -344,40 +384,60 @@ __global__ void __launch_bounds__(TC::NT)
                    y0 + p.h[1] - R, zz);
   };
   const int zi0 = zb - WARM;
-  // plane sequence number of z: q(z) = z - zb + R; iteration zi issues q(zi + U + PD)
+  // Plane sequence number q(z) = z - (zb - R), ring slot q % NSLOT, barrier
+  // phase (q / NSLOT) & 1.  Iteration zi issues plane q(zi + U + PD), waits
+  // for q(zi + U), reads the field planes zi + L .. zi + U and the staged
+  // planes zi - RS .. zi + RS, and writes staged plane zi + RS.  The slots and
+  // phases are advanced by one per iteration (no divisions), and the planes
+  // read are kept as windows of pointers shifted by one plane per iteration.
+  constexpr int NPW = U - L + 1;                // field planes read per iteration
+  constexpr int NSW = NS > 0 ? 2 * RS + 1 : 1;  // staged planes read per iteration
+  const int q0 = zi0 - (zb - R);                // q of plane zi0 (>= 0)
   if (tid == 0) {
-    const int pro = min(zi0 + U + PD - (zb - R), nplanes);
+    const int pro = min(q0 + U + PD, nplanes);
     for (int q = 0; q < pro; ++q) issue(q);
   }
+  // every plane the first iteration reads except the newest, which the first
+  // iteration waits for like any other
+  bool bad0 = false;
+  for (int q = 0; q < q0 + U; ++q) bad0 |= !tma::mbar_wait(&bars[q % NSLOT], (q / NSLOT) & 1);
+
+  const T* const fend = fbuf + NSLOT * PLANE;
+  const T* pw[NPW];  // field plane zi + L + j, field 0
+  pw[0] = fbuf + (((q0 + L) % NSLOT + NSLOT) % NSLOT) * PLANE;
+#pragma unroll
+  for (int j = 1; j < NPW; ++j) pw[j] = pw[j - 1] + PLANE == fend ? fbuf : pw[j - 1] + PLANE;
+  const T* ps[NSW];  // staged plane zi - RS + j, operand 0
+  if constexpr (NS > 0) {
+    // staged planes count from zb - RS: plane zi0 - RS + j is number j - 2 RS
+    const T* const send = sbuf + NSR * SPL;
+    ps[0] = sbuf + (((-2 * RS) % NSR + NSR) % NSR) * SPL;
+#pragma unroll
+    for (int j = 1; j < NSW; ++j) ps[j] = ps[j - 1] + SPL == send ? sbuf : ps[j - 1] + SPL;
+  }
+  int qw = q0 + U, wslot = qw % NSLOT, wph = (qw / NSLOT) & 1;  // plane waited for
+  int qn = q0 + U + PD, nslot = qn % NSLOT;                      // plane issued
 
   double msum = 0.0;
-  // ring slot of plane zi (field ring) and of staged plane zi (stage ring),
-  // advanced by one per iteration instead of divided out
-  int zslot = ((zi0 - (zb - R)) % NSLOT + NSLOT) % NSLOT;
-  int sslot0 = NS > 0 ? ((zi0 - (zb - RS)) % (NSR > 0 ? NSR : 1) + NSR) % (NSR > 0 ? NSR : 1) : 0;
-
-  for (int zi = zi0; zi < ze; ++zi, zslot = wrap<NSLOT>(zslot, 1),
-           sslot0 = NS > 0 ? wrap<(NSR > 0 ? NSR : 1)>(sslot0, 1) : 0) {
-    const int qn = zi + U + PD - (zb - R);
-    if (tid == 0 && qn < nplanes) issue(qn);
-    bool bad = false;
-    const int qw = zi + U - (zb - R);
-    if (zi == zi0) {
-      for (int q = 0; q <= qw; ++q) bad |= !tma::mbar_wait(&bars[q % NSLOT], (q / NSLOT) & 1);
-    } else {
-      bad = !tma::mbar_wait(&bars[wrap<NSLOT>(zslot, U)], (qw / NSLOT) & 1);
+  for (int zi = zi0; zi < ze; ++zi) {
+    if (tid == 0 && qn < nplanes) {
+      tma::mbar_arrive_expect_tx(&bars[nslot], TXB);
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+        tma::load_3d(fbuf + (f * NSLOT + nslot) * PLANE, maps + f, &bars[nslot],
+                     x0 + p.h[0] - HXA, y0 + p.h[1] - R, zb - R + qn + p.h[2]);
     }
+    bool bad = !tma::mbar_wait(&bars[wslot], wph);
+    if (zi == zi0) bad |= bad0;
 
     if constexpr (NS > 0) {
       using CS = Ctx<T, W, !EXACT, 3, LP, GP, BP, NF, 2 * RI + 1, RI, PW, 1, 1, 0, SW>;
-      T* sdst = sbuf + wrap<NSR>(sslot0, RS) * SPL;
+      T* sdst = const_cast<T*>(ps[NSW - 1]);
       CS c0;
-      c0.base = fbuf;
 #pragma unroll
       for (int f = 0; f < NF; ++f)
 #pragma unroll
-        for (int dz = -RI; dz <= RI; ++dz)
-          c0.fo[f][dz + RI] = (f * NSLOT + wrap<NSLOT>(zslot, RS + dz)) * PLANE;
+        for (int dz = -RI; dz <= RI; ++dz) c0.fo[f][dz + RI] = pw[RS + dz - L] + f * NSLOT * PLANE;
       c0.divh2 = vdivh2;
       c0.divh3 = vdivh3;
       c0.divh4 = vdivh4;
@@ -395,17 +455,21 @@ __global__ void __launch_bounds__(TC::NT)
         o[0] = eval(m.s0, ctx);
         if constexpr (NS > 1) o[1] = eval(m.s1, ctx);
       };
-      V sv[SPT + 1][SO];
+      V sv[SPT + NX1][SO];
 #pragma unroll
       for (int k = 0; k < SPT; ++k) cell(row0 + k, txt, sv[k]);
-      if (xsr >= 0) cell(xsr, xsc, sv[SPT]);
+#pragma unroll
+      for (int j = 0; j < NX; ++j)
+        if (xsr[j] >= 0) cell(xsr[j], xsc[j], sv[SPT + j]);
       auto put = [&](int sr, int c, const V (&o)[SO]) {
         *reinterpret_cast<V*>(sdst + sr * SW + c * W) = o[0];
         if constexpr (NS > 1) *reinterpret_cast<V*>(sdst + NSR * SPL + sr * SW + c * W) = o[1];
       };
 #pragma unroll
       for (int k = 0; k < SPT; ++k) put(row0 + k, txt, sv[k]);
-      if (xsr >= 0) put(xsr, xsc, sv[SPT]);
+#pragma unroll
+      for (int j = 0; j < NX; ++j)
+        if (xsr[j] >= 0) put(xsr[j], xsc[j], sv[SPT + j]);
     }
 
     // the one barrier of the iteration: planes waited for, stages written
@@ -422,20 +486,17 @@ __global__ void __launch_bounds__(TC::NT)
       using CO = Ctx<T, W, !EXACT, 3, LP, GP, BP, NF, 2 * RD + 1, RD, PW, NS,
                      (NS > 0 ? 2 * RS + 1 : 1), (NS > 0 ? RS : 0), SW>;
       CO c0;
-      c0.base = fbuf;
       const int cell = (row0 + R) * PW + txt * W + HXA;
 #pragma unroll
       for (int f = 0; f < NF; ++f)
 #pragma unroll
-        for (int dz = -RD; dz <= RD; ++dz)
-          c0.fo[f][dz + RD] = (f * NSLOT + wrap<NSLOT>(zslot, dz)) * PLANE + cell;
+        for (int dz = -RD; dz <= RD; ++dz) c0.fo[f][dz + RD] = pw[dz - L] + f * NSLOT * PLANE + cell;
       if constexpr (NS > 0) {
-        const int scell = int(sbuf - fbuf) + (row0 + RS) * SW + txt * W + RSA;
+        const int scell = (row0 + RS) * SW + txt * W + RSA;
 #pragma unroll
         for (int k = 0; k < NS; ++k)
 #pragma unroll
-          for (int dz = -RS; dz <= RS; ++dz)
-            c0.so[k][dz + RS] = (k * NSR + wrap<NSR>(sslot0, dz)) * SPL + scell;
+          for (int dz = -RS; dz <= RS; ++dz) c0.so[k][dz + RS] = ps[dz + RS] + k * NSR * SPL + scell;
       }
       c0.divh2 = vdivh2;
       c0.divh3 = vdivh3;
@@ -464,19 +525,21 @@ __global__ void __launch_bounds__(TC::NT)
       }
       const long long zoff = (long long)(z + p.h[2]) * p.plane;
       const long long zo = image_offset(p.per[2], z, 1, p.n[2], R, p.plane);
-      if (simple && zo == 0) {
+      if (plain && zo == 0) {
 #pragma unroll
         for (int k = 0; k < SPT; ++k)
 #pragma unroll
           for (int f = 0; f < NF; ++f) *reinterpret_cast<V*>(orow[k][f] + zoff) = nv[k][f];
       } else {
+        // a tile at a face or the end of the domain: every group and its
+        // images as predicated stores (no divergence); a group cut by the end
+        // of a row element by element
 #pragma unroll
         for (int k = 0; k < SPT; ++k) {
-          if (!rowin[k]) continue;
-          if (vec_ok) {
 #pragma unroll
-            for (int f = 0; f < NF; ++f) put_images(orow[k][f] + zoff, nv[k][f], xo, yo[k], zo);
-          } else {
+          for (int f = 0; f < NF; ++f)
+            put_images_pred(orow[k][f] + zoff, nv[k][f], rowin[k] && vec_ok, xo, yo[k], zo);
+          if (ragged && rowin[k]) {
 #pragma unroll
             for (int f = 0; f < NF; ++f)
               store_group<T, W, 3, R>(p.out[inst * NF + f], x, y0 + row0 + k, z, nv[k][f], p.n,
@@ -490,6 +553,28 @@ __global__ void __launch_bounds__(TC::NT)
           if (rowin[k]) msum += vsum<T, W>(nv[k][0], x, p.n[0]);
       }
     }
+
+    // advance the windows, the waited-for and the issued plane by one
+    {
+      const T* nw = pw[NPW - 1] + PLANE == fend ? fbuf : pw[NPW - 1] + PLANE;
+#pragma unroll
+      for (int j = 0; j < NPW - 1; ++j) pw[j] = pw[j + 1];
+      pw[NPW - 1] = nw;
+    }
+    if constexpr (NS > 0) {
+      const T* const send = sbuf + NSR * SPL;
+      const T* nw = ps[NSW - 1] + SPL == send ? sbuf : ps[NSW - 1] + SPL;
+#pragma unroll
+      for (int j = 0; j < NSW - 1; ++j) ps[j] = ps[j + 1];
+      ps[NSW - 1] = nw;
+    }
+    ++qw;
+    if (++wslot == NSLOT) {
+      wslot = 0;
+      wph ^= 1;
+    }
+    ++qn;
+    if (++nslot == NSLOT) nslot = 0;
   }
   __syncthreads();
 
@@ -526,18 +611,20 @@ struct Fd2 {
   static constexpr int SW = TX + 2 * RSA, SH = TY + 2 * RS, SPL = ceil_to(SW * SH, 32);
   static constexpr int SWC = SW / W, XC = 2 * RSA / W;
   static constexpr int NE = 2 * RS * SWC + TY * XC;
+  static constexpr int NX = (NE + NT - 1) / NT, NX1 = NX > 0 ? NX : 1;
   static constexpr size_t SMEM =
       256 + sizeof(T) * (size_t(NQ) * NF * PLANE + size_t(2) * NS * SPL);
   static_assert(NQ <= 16, "barrier header holds 16 slots");
   static_assert(PW <= 256 && PH <= 256, "TMA box limit");
   static_assert((PW * sizeof(T)) % 16 == 0, "TMA box rows must be whole 16-byte units");
-  static_assert(NE <= NT, "one extra stage cell per thread at most");
+  static_assert(NX <= 4, "extra stage cells per thread");
 };
 
 // staged operands of model M for one tile
 template <class K, class M, class T, int LP, int GP, int BP>
 __device__ __forceinline__ void fd2_stage(const M& m, const Inst2<T>& ip, const T* fbuf, T* sbuf,
-                                          int slot, int xsr, int xsc) {
+                                          int slot, const int (&xsr)[K::NX1],
+                                          const int (&xsc)[K::NX1]) {
   constexpr int SPT = K::SPT, W = K::W, TXT = K::TXT, NF = K::NF, R = K::R, RS = K::RS,
                 RSA = K::RSA, HXA = K::HXA, PW = K::PW, PLANE = K::PLANE, SW = K::SW;
   constexpr int NS = M::ns;
@@ -549,9 +636,8 @@ __device__ __forceinline__ void fd2_stage(const M& m, const Inst2<T>& ip, const 
 #pragma unroll
   for (int i = 0; i < 8; ++i) coef[i] = ip.coef[i];
   CS c0;
-  c0.base = fbuf;
 #pragma unroll
-  for (int f = 0; f < NF; ++f) c0.fo[f][0] = (slot * NF + f) * PLANE;
+  for (int f = 0; f < NF; ++f) c0.fo[f][0] = fbuf + (slot * NF + f) * PLANE;
   c0.divh2 = V(ip.divh2);
   c0.divh3 = V(ip.divh3);
   c0.divh4 = V(ip.divh4);
@@ -564,17 +650,21 @@ __device__ __forceinline__ void fd2_stage(const M& m, const Inst2<T>& ip, const 
     o[0] = eval(m.s0, ctx);
     if constexpr (NS > 1) o[1] = eval(m.s1, ctx);
   };
-  V sv[SPT + 1][SO];
+  V sv[SPT + K::NX1][SO];
 #pragma unroll
   for (int k = 0; k < SPT; ++k) cell(row0 + k, txt, sv[k]);
-  if (xsr >= 0) cell(xsr, xsc, sv[SPT]);
+#pragma unroll
+  for (int j = 0; j < K::NX; ++j)
+    if (xsr[j] >= 0) cell(xsr[j], xsc[j], sv[SPT + j]);
   auto put = [&](int sr, int c, const V (&o)[SO]) {
     *reinterpret_cast<V*>(sbuf + sr * SW + c * W) = o[0];
     if constexpr (NS > 1) *reinterpret_cast<V*>(sbuf + K::SPL + sr * SW + c * W) = o[1];
   };
 #pragma unroll
   for (int k = 0; k < SPT; ++k) put(row0 + k, txt, sv[k]);
-  if (xsr >= 0) put(xsr, xsc, sv[SPT]);
+#pragma unroll
+  for (int j = 0; j < K::NX; ++j)
+    if (xsr[j] >= 0) put(xsr[j], xsc[j], sv[SPT + j]);
 }
 
 // right-hand sides, Euler update and stores of model M for one tile
@@ -582,7 +672,7 @@ template <class K, class M, class T, int LP, int GP, int BP>
 __device__ __forceinline__ void fd2_out(const Step2Params<T>& p, const M& m, const Inst2<T>& ip,
                                         int ii, const T* fbuf, const T* sbuf, int slot, int x0,
                                         int y0, double& msum) {
-  constexpr int SPT = K::SPT, W = K::W, TXT = K::TXT, NF = K::NF, R = K::R, RS = K::RS,
+  constexpr int TX = K::TX, TY = K::TY, SPT = K::SPT, W = K::W, TXT = K::TXT, NF = K::NF, R = K::R, RS = K::RS,
                 RSA = K::RSA, HXA = K::HXA, PW = K::PW, PLANE = K::PLANE, SW = K::SW;
   constexpr int NS = M::ns;
   using V = vec_t<T, W>;
@@ -594,14 +684,13 @@ __device__ __forceinline__ void fd2_out(const Step2Params<T>& p, const M& m, con
   const long long pitch = ip.pitch;
   using CO = Ctx<T, W, !K::exact, 2, LP, GP, BP, NF, 1, 0, PW, NS, 1, 0, SW>;
   CO c0;
-  c0.base = fbuf;
   const int cell = (row0 + R) * PW + txt * W + HXA;
 #pragma unroll
-  for (int f = 0; f < NF; ++f) c0.fo[f][0] = (slot * NF + f) * PLANE + cell;
+  for (int f = 0; f < NF; ++f) c0.fo[f][0] = fbuf + (slot * NF + f) * PLANE + cell;
   if constexpr (NS > 0) {
     const int scell = int(sbuf - fbuf) + (row0 + RS) * SW + txt * W + RSA;
 #pragma unroll
-    for (int k = 0; k < NS; ++k) c0.so[k][0] = k * K::SPL + scell;
+    for (int k = 0; k < NS; ++k) c0.so[k][0] = fbuf + k * K::SPL + scell;
   }
   const V vdt(ip.dt);
   c0.divh2 = V(ip.divh2);
@@ -635,9 +724,12 @@ __device__ __forceinline__ void fd2_out(const Step2Params<T>& p, const M& m, con
 #pragma unroll
   for (int f = 0; f < NF; ++f) out[f] = p.out[ii * NF + f];
   const int yr0 = y0 + row0;
-  const bool simple = vec_ok && xo == 0 && yr0 + SPT <= n1 &&
-                      !(ip.per[1] && (yr0 < R || yr0 + SPT > n1 - R));
-  if (simple) {
+  // the whole tile inside the domain, away from every periodic face, in whole
+  // vectors: straight-line stores (the same for every thread of the block)
+  const bool plain = (n0 % W == 0) && x0 + TX <= n0 && y0 + TY <= n1 &&
+                     (!ip.per[0] || (x0 >= R && x0 + TX <= n0 - R)) &&
+                     (!ip.per[1] || (y0 >= R && y0 + TY <= n1 - R));
+  if (plain) {
     T* b0 = nullptr;
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
@@ -646,16 +738,20 @@ __device__ __forceinline__ void fd2_out(const Step2Params<T>& p, const M& m, con
       for (int k = 0; k < SPT; ++k) *reinterpret_cast<V*>(b0 + k * pitch) = nv[k][f];
     }
   } else {
+    // a tile at a face or the end of the domain: whole groups and their
+    // images as predicated stores (no divergence); a group cut by the end of
+    // a row element by element
+    const bool ragged = x < n0 && !vec_ok;
 #pragma unroll
     for (int k = 0; k < SPT; ++k) {
       const int y = y0 + row0 + k;
-      if (x >= n0 || y >= n1) continue;
-      if (vec_ok) {
-        const long long yo = image_offset(ip.per[1], y, 1, n1, R, pitch);
+      const bool in = x < n0 && y < n1;
+      const long long yo = image_offset(ip.per[1], y, 1, n1, R, pitch);
 #pragma unroll
-        for (int f = 0; f < NF; ++f)
-          put_images(out[f] + (long long)(y + p.hy) * pitch + x + p.hx, nv[k][f], xo, yo, 0LL);
-      } else {
+      for (int f = 0; f < NF; ++f)
+        put_images_pred(out[f] + (long long)(y + p.hy) * pitch + x + p.hx, nv[k][f],
+                        in && vec_ok, xo, yo, 0LL);
+      if (ragged && in) {
 #pragma unroll
         for (int f = 0; f < NF; ++f)
           store_group<T, W, 2, R>(out[f], x, y, 0, nv[k][f], n3, h, per3, pitch, 0);
@@ -687,19 +783,8 @@ __global__ void __launch_bounds__(TC::NT)
   __shared__ double red[32];
   const int tid = threadIdx.x;
 
-  int xsr = -1, xsc = 0;
-  if constexpr (NS > 0) {
-    if (tid < NE) {
-      if (tid < 2 * RS * SWC) {
-        xsr = TY + tid / SWC;
-        xsc = tid % SWC;
-      } else {
-        const int e = tid - 2 * RS * SWC;
-        xsr = e / XC;
-        xsc = TXT + e % XC;
-      }
-    }
-  }
+  int xsr[K::NX1], xsc[K::NX1];
+  extra_cells<NE, NT, K::NX, TY, RS, SWC, XC, TXT>(tid, xsr, xsc);
 
   auto fetch = [&]() -> int2 {
     const int t = atomicAdd(&p.ctr[0], 1);

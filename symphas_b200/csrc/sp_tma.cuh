@@ -49,12 +49,27 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`: try_wait already suspends the
-// thread in hardware for a while; give up after about 2^31 SM cycles (~1 s).
+// try_wait with a suspend-time hint (ns): the thread sleeps in hardware until
+// the phase completes or the hint expires, instead of re-issuing the poll
+__device__ __forceinline__ bool mbar_try_wait_for(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(saddr(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for phase `parity` of `bar`: each try sleeps up to 1 ms in
+// hardware (woken when the phase completes); give up after about 2^31 SM
+// cycles (~1 s).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity))
+  while (!mbar_try_wait_for(bar, parity, 1000000u))
     if (clock64() - t0 > (1LL << 31)) return false;
   return true;
 }
