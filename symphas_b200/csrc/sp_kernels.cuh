@@ -259,11 +259,18 @@ struct Fd3 {
   static constexpr int RSA = G::RSA, HXA = G::HXA;
   static constexpr int PW = TX + 2 * HXA, PH = TY + 2 * R;
   static constexpr int PLANE = ceil_to(PW * PH, 128 / (int)sizeof(T));
-  // one barrier per plane: each ring keeps one spare plane so a fast thread
-  // may fill it while a slow one still reads the previous iteration's planes
-  static constexpr int NSLOT = (U - L + 1) + 1 + PD;
+  // One barrier per plane, at the end of the iteration.  The output of plane
+  // zi reads staged planes zi - RS .. zi + RS: the in-plane neighbours only at
+  // zi (staged by the previous iteration, behind its barrier), and the other
+  // planes only at the thread's own sites, which the thread itself staged.  So
+  // the stage of plane zi + RS and the output of plane zi need no barrier
+  // between them, and the stage ring holds just the 2 RS + 1 planes read.
+  // Field ring: the U - L planes the next iteration still reads and PD in
+  // flight; the plane issued after the barrier reuses the slot of plane zi + L,
+  // which no later iteration reads.
+  static constexpr int NSLOT = (U - L) + PD;
   static constexpr int SW = TX + 2 * RSA, SH = TY + 2 * RS, SPL = ceil_to(SW * SH, 32);
-  static constexpr int NSR = NS > 0 ? 2 * RS + 2 : 0;
+  static constexpr int NSR = NS > 0 ? 2 * RS + 1 : 0;
   static constexpr int SWC = SW / W;        // column groups of a stage row
   static constexpr int XC = 2 * RSA / W;    // extra column groups left and right
   static constexpr int NE = 2 * RS * SWC + TY * XC;  // stage cells beyond one per row group
@@ -271,16 +278,23 @@ struct Fd3 {
   static constexpr size_t SMEM =
       256 + sizeof(T) * (size_t(NF) * NSLOT * PLANE + size_t(NS) * NSR * SPL);
   static_assert(U == R, "the newest plane needed is R ahead");
-  static_assert(R - WARM <= 2 - L, "prologue planes fit in the ring");
+  static_assert(R - WARM + L <= 0, "prologue planes fit in the ring");
+  static_assert(PD >= 1, "at least one plane in flight");
+  // staged planes are read off the own site only at z offsets other than 0
+  // (the 7-point Laplacian of the fused form)
+  static_assert(NS == 0 || LP == 7, "staged operands under the 7-point Laplacian only");
   static_assert(NSLOT <= 32, "barrier header holds 32 slots");
   static_assert(PW <= 256 && PH <= 256, "TMA box limit");
   static_assert((PW * sizeof(T)) % 16 == 0, "TMA box rows must be whole 16-byte units");
   static_assert(NX <= 4, "extra stage cells per thread");
 };
 
-// the stage cells of a tile beyond the row groups of its threads: the RS rows
-// below the tile (all column groups), then the XC column groups right of each
-// row; thread tid takes cells tid, tid + NT, ... (row -1 marks none)
+// Stage cells of a tile.  Each thread stages the cells of its own output
+// sites (stage row row0 + k + RS, column group txt + RSA / W), so a staged
+// value at the thread's own site is one the thread wrote itself.  The ring
+// around them -- the RS rows above and below (every column group) and the
+// XC / 2 column groups left and right of each inner row -- is shared out:
+// thread tid takes ring cells tid, tid + NT, ... (row -1 marks none).
 template <int NE, int NT, int NX, int TY, int RS, int SWC, int XC, int TXT>
 __device__ __forceinline__ void extra_cells(int tid, int (&xsr)[NX > 0 ? NX : 1],
                                             int (&xsc)[NX > 0 ? NX : 1]) {
@@ -292,12 +306,13 @@ __device__ __forceinline__ void extra_cells(int tid, int (&xsr)[NX > 0 ? NX : 1]
     if constexpr (NE > 0) {
       if (e >= NE) continue;
       if (e < 2 * RS * SWC) {
-        xsr[j] = TY + e / SWC;
+        const int r = e / SWC;
+        xsr[j] = r < RS ? r : TY + r;
         xsc[j] = e % SWC;
       } else {
-        const int e2 = e - 2 * RS * SWC;
-        xsr[j] = e2 / XC;
-        xsc[j] = TXT + e2 % XC;
+        const int e2 = e - 2 * RS * SWC, cc = e2 % XC;
+        xsr[j] = RS + e2 / XC;
+        xsc[j] = cc < XC / 2 ? cc : TXT + cc;
       }
     }
   }
@@ -385,8 +400,8 @@ __global__ void __launch_bounds__(TC::NT)
   };
   const int zi0 = zb - WARM;
   // Plane sequence number q(z) = z - (zb - R), ring slot q % NSLOT, barrier
-  // phase (q / NSLOT) & 1.  Iteration zi issues plane q(zi + U + PD), waits
-  // for q(zi + U), reads the field planes zi + L .. zi + U and the staged
+  // phase (q / NSLOT) & 1.  Iteration zi waits for q(zi + U), issues plane
+  // q(zi + U + PD) after its barrier, reads the field planes zi + L .. zi + U and the staged
   // planes zi - RS .. zi + RS, and writes staged plane zi + RS.  The slots and
   // phases are advanced by one per iteration (no divisions), and the planes
   // read are kept as windows of pointers shifted by one plane per iteration.
@@ -420,13 +435,6 @@ __global__ void __launch_bounds__(TC::NT)
 
   double msum = 0.0;
   for (int zi = zi0; zi < ze; ++zi) {
-    if (tid == 0 && qn < nplanes) {
-      tma::mbar_arrive_expect_tx(&bars[nslot], TXB);
-#pragma unroll
-      for (int f = 0; f < NF; ++f)
-        tma::load_3d(fbuf + (f * NSLOT + nslot) * PLANE, maps + f, &bars[nslot],
-                     x0 + p.h[0] - HXA, y0 + p.h[1] - R, zb - R + qn + p.h[2]);
-    }
     bool bad = !tma::mbar_wait(&bars[wslot], wph);
     if (zi == zi0) bad |= bad0;
 
@@ -457,7 +465,7 @@ __global__ void __launch_bounds__(TC::NT)
       };
       V sv[SPT + NX1][SO];
 #pragma unroll
-      for (int k = 0; k < SPT; ++k) cell(row0 + k, txt, sv[k]);
+      for (int k = 0; k < SPT; ++k) cell(row0 + k + RS, txt + RSA / W, sv[k]);
 #pragma unroll
       for (int j = 0; j < NX; ++j)
         if (xsr[j] >= 0) cell(xsr[j], xsc[j], sv[SPT + j]);
@@ -466,19 +474,10 @@ __global__ void __launch_bounds__(TC::NT)
         if constexpr (NS > 1) *reinterpret_cast<V*>(sdst + NSR * SPL + sr * SW + c * W) = o[1];
       };
 #pragma unroll
-      for (int k = 0; k < SPT; ++k) put(row0 + k, txt, sv[k]);
+      for (int k = 0; k < SPT; ++k) put(row0 + k + RS, txt + RSA / W, sv[k]);
 #pragma unroll
       for (int j = 0; j < NX; ++j)
         if (xsr[j] >= 0) put(xsr[j], xsc[j], sv[SPT + j]);
-    }
-
-    // the one barrier of the iteration: planes waited for, stages written
-    if (__syncthreads_or(bad)) {
-      if (tid == 0) {
-        atomicExch(p.err, KERR_TMA_TIMEOUT);
-        tma::drain(bars, NSLOT, zi == zi0 ? 0 : qw, min(qn, nplanes - 1));
-      }
-      return;
     }
 
     if (zi >= zb) {
@@ -552,6 +551,23 @@ __global__ void __launch_bounds__(TC::NT)
         for (int k = 0; k < SPT; ++k)
           if (rowin[k]) msum += vsum<T, W>(nv[k][0], x, p.n[0]);
       }
+    }
+
+    // the one barrier of the iteration: staged plane zi + RS written, every
+    // read of this iteration done
+    if (__syncthreads_or(bad)) {
+      if (tid == 0) {
+        atomicExch(p.err, KERR_TMA_TIMEOUT);
+        tma::drain(bars, NSLOT, zi == zi0 ? 0 : qw, min(qn - 1, nplanes - 1));
+      }
+      return;
+    }
+    if (tid == 0 && qn < nplanes) {
+      tma::mbar_arrive_expect_tx(&bars[nslot], TXB);
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+        tma::load_3d(fbuf + (f * NSLOT + nslot) * PLANE, maps + f, &bars[nslot],
+                     x0 + p.h[0] - HXA, y0 + p.h[1] - R, zb - R + qn + p.h[2]);
     }
 
     // advance the windows, the waited-for and the issued plane by one
@@ -652,7 +668,7 @@ __device__ __forceinline__ void fd2_stage(const M& m, const Inst2<T>& ip, const 
   };
   V sv[SPT + K::NX1][SO];
 #pragma unroll
-  for (int k = 0; k < SPT; ++k) cell(row0 + k, txt, sv[k]);
+  for (int k = 0; k < SPT; ++k) cell(row0 + k + RS, txt + RSA / W, sv[k]);
 #pragma unroll
   for (int j = 0; j < K::NX; ++j)
     if (xsr[j] >= 0) cell(xsr[j], xsc[j], sv[SPT + j]);
@@ -661,7 +677,7 @@ __device__ __forceinline__ void fd2_stage(const M& m, const Inst2<T>& ip, const 
     if constexpr (NS > 1) *reinterpret_cast<V*>(sbuf + K::SPL + sr * SW + c * W) = o[1];
   };
 #pragma unroll
-  for (int k = 0; k < SPT; ++k) put(row0 + k, txt, sv[k]);
+  for (int k = 0; k < SPT; ++k) put(row0 + k + RS, txt + RSA / W, sv[k]);
 #pragma unroll
   for (int j = 0; j < K::NX; ++j)
     if (xsr[j] >= 0) put(xsr[j], xsc[j], sv[SPT + j]);

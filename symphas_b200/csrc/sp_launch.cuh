@@ -138,13 +138,13 @@ SP_FACTORY(MF_OP_LAPCUBE, models::op_lapcube())
 namespace sp {
 template <class T> struct Tiles;
 template <> struct Tiles<float> {
-  using D3 = TileCfg<64, 16, 2, 4, 2>;
+  using D3 = TileCfg<64, 16, 4, 3, 2>;
   using D2 = TileCfg<128, 16, 4, 3, 2>;
   // further shapes the autotuner tries for the headline (fused FP32) kernels
   using D3b = TileCfg<64, 32, 4, 2, 2>;
-  using D3c = TileCfg<64, 16, 4, 4, 2>;
+  using D3c = TileCfg<128, 16, 4, 3, 2>;
   using D3d = TileCfg<128, 16, 4, 2, 2>;
-  using D3e = TileCfg<64, 16, 2, 2, 2>;
+  using D3e = TileCfg<64, 16, 2, 3, 2>;
   using D3f = TileCfg<64, 16, 4, 2, 2>;
   using C3a = TileCfg<64, 16, 4, 2, 2>;  // conserved-pattern kernel shapes
   using C3b = TileCfg<64, 16, 2, 2, 2>;
