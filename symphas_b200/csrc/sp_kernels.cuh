@@ -623,7 +623,7 @@ struct Fd2 {
   static constexpr int RSA = G::RSA, HXA = G::HXA;
   static constexpr int PW = TX + 2 * HXA, PH = TY + 2 * R;
   static constexpr int PLANE = ceil_to(PW * PH, 128 / (int)sizeof(T));
-  static constexpr int NQ = PD + 2;  // tile slots: PD in flight, the current and the previous
+  static constexpr int NQ = PD + 2;  // tile slots: PD in flight, the one staged, the one output
   static constexpr int SW = TX + 2 * RSA, SH = TY + 2 * RS, SPL = ceil_to(SW * SH, 32);
   static constexpr int SWC = SW / W, XC = 2 * RSA / W;
   static constexpr int NE = 2 * RS * SWC + TY * XC;
@@ -817,57 +817,92 @@ __global__ void __launch_bounds__(TC::NT)
                    x0 + p.hx - HXA, y0 + p.hy - R);
   };
 
+  // Tile j of this CTA's sequence lives in ring slot j % NQ (barrier phase
+  // (j / NQ) & 1) and stages into copy j & 1 of the stage buffer.  Iteration
+  // it stages tile it + 1 and writes the output of tile it, staged by the
+  // previous iteration: the two are independent, so one barrier per tile, at
+  // the end of the iteration, orders everything.  The ring holds tiles it and
+  // it + 1 and PD in flight; iteration it issues tile it + 1 + PD into the slot
+  // of tile it - 1, which every thread finished with before the last barrier.
+  auto item_at = [&](int j) -> int2 {
+    const volatile int* v = reinterpret_cast<volatile int*>(&items[j % NQ]);
+    return make_int2(v[0], v[1]);
+  };
+  auto stage = [&](int2 t, int j) {
+    if constexpr (NS > 0) {
+      const Inst2<T>& ip = p.inst[t.x];
+      T* sb = sbuf + (j & 1) * NS * K::SPL;
+      if (ip.kind == 0) {
+        if constexpr (M0::ns > 0)
+          fd2_stage<K, M0, T, LP, GP, BP>(m0, ip, fbuf, sb, j % NQ, xsr, xsc);
+      } else {
+        if constexpr (M1::ns > 0)
+          fd2_stage<K, M1, T, LP, GP, BP>(m1, ip, fbuf, sb, j % NQ, xsr, xsc);
+      }
+    }
+  };
+  // error path: record, wait (bounded) for tiles first .. first + PD still in
+  // flight, leave
+  auto give_up = [&](int first) {
+    if (tid == 0) {
+      atomicExch(p.err, KERR_TMA_TIMEOUT);
+      for (int j = first; j <= first + PD; ++j)
+        if (item_at(j).x >= 0) tma::mbar_wait(&bars[j % NQ], (j / NQ) & 1);
+    }
+  };
+
   if (tid == 0) {
     for (int s = 0; s < NQ; ++s) tma::mbar_init(&bars[s], 1);
     tma::fence_barrier_init();
-    for (int s = 0; s < PD; ++s) {
-      const int2 it = fetch();
-      items[s] = it;
-      if (it.x >= 0) issue(it, s);
+    for (int s = 0; s <= PD; ++s) {
+      const int2 t = fetch();
+      items[s] = t;
+      if (t.x >= 0) issue(t, s);
     }
   }
   __syncthreads();
+  {
+    const int2 t0 = item_at(0);
+    bool bad = false;
+    if (t0.x >= 0) {
+      bad = !tma::mbar_wait(&bars[0], 0);
+      if (!bad) stage(t0, 0);
+    }
+    if (__syncthreads_or(bad)) {
+      give_up(0);
+      return;
+    }
+  }
 
   double msum = 0.0;
   for (int it = 0;; ++it) {
-    const int slot = it % NQ;
-    const volatile int* vi = reinterpret_cast<volatile int*>(&items[slot]);
-    const int2 cur = make_int2(vi[0], vi[1]);
+    const int2 cur = item_at(it);
     if (cur.x < 0) break;
+    const int2 nxt = item_at(it + 1);
     if (tid == 0) {
-      const int2 nxt = fetch();
-      const int ns = (it + PD) % NQ;
-      items[ns] = nxt;
-      if (nxt.x >= 0) issue(nxt, ns);
+      const int2 t = fetch();
+      const int ns = (it + 1 + PD) % NQ;
+      items[ns] = t;
+      if (t.x >= 0) issue(t, ns);
     }
-    const bool bad = !tma::mbar_wait(&bars[slot], (it / NQ) & 1);
-    const Inst2<T>& ip = p.inst[cur.x];
-    T* sb = sbuf + (it & 1) * (NS > 0 ? NS : 1) * K::SPL;
-    if constexpr (NS > 0) {
-      if (!bad) {
-        if (ip.kind == 0) {
-          if constexpr (M0::ns > 0) fd2_stage<K, M0, T, LP, GP, BP>(m0, ip, fbuf, sb, slot, xsr, xsc);
-        } else {
-          if constexpr (M1::ns > 0) fd2_stage<K, M1, T, LP, GP, BP>(m1, ip, fbuf, sb, slot, xsr, xsc);
-        }
-      }
+    bool bad = false;
+    if (nxt.x >= 0) {
+      bad = !tma::mbar_wait(&bars[(it + 1) % NQ], ((it + 1) / NQ) & 1);
+      if (!bad) stage(nxt, it + 1);
+    }
+    {
+      const Inst2<T>& ip = p.inst[cur.x];
+      const T* sb = sbuf + (it & 1) * (NS > 0 ? NS : 1) * K::SPL;
+      const int x0 = (cur.y % ip.ntx) * TX, y0 = (cur.y / ip.ntx) * TY;
+      if (ip.kind == 0)
+        fd2_out<K, M0, T, LP, GP, BP>(p, m0, ip, cur.x, fbuf, sb, it % NQ, x0, y0, msum);
+      else
+        fd2_out<K, M1, T, LP, GP, BP>(p, m1, ip, cur.x, fbuf, sb, it % NQ, x0, y0, msum);
     }
     if (__syncthreads_or(bad)) {
-      if (tid == 0) {
-        atomicExch(p.err, KERR_TMA_TIMEOUT);
-        // tiles it .. it + PD were issued into distinct slots (PD < NQ)
-        for (int j = it; j <= it + PD; ++j) {
-          const volatile int* vj = reinterpret_cast<volatile int*>(&items[j % NQ]);
-          if (vj[0] >= 0) tma::mbar_wait(&bars[j % NQ], (j / NQ) & 1);
-        }
-      }
+      give_up(it + 1);
       return;
     }
-    const int x0 = (cur.y % ip.ntx) * TX, y0 = (cur.y / ip.ntx) * TY;
-    if (ip.kind == 0)
-      fd2_out<K, M0, T, LP, GP, BP>(p, m0, ip, cur.x, fbuf, sb, slot, x0, y0, msum);
-    else
-      fd2_out<K, M1, T, LP, GP, BP>(p, m1, ip, cur.x, fbuf, sb, slot, x0, y0, msum);
   }
   __syncthreads();
   if (tid == 0) {

@@ -2,6 +2,7 @@
 the time per step.  Used for timing and for profiling single launches:
 
     python -m symphas_b200.run --model B --dim 3 --n 256 --dtype f32 --steps 8
+    python -m symphas_b200.run --ensemble 128 --steps 8     (2D AMK/BMK members)
 
 Steps are launched one at a time (no CUDA graph), so a profiler sees each
 fused-step launch separately.
@@ -27,9 +28,14 @@ def main(argv=None):
     ap.add_argument("--dt", type=float, default=0.005)
     ap.add_argument("--h", type=float, default=1.0)
     ap.add_argument("--coeff", type=float, nargs="*", default=[])
+    ap.add_argument("--ensemble", type=int, default=0,
+                    help="run an ensemble of this many 2D members (sides 64..1024, models AMK "
+                         "and BMK, FP32 fused) instead of one model")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the fastest tile shape first (its launches come before the steps)")
     a = ap.parse_args(argv)
+    if a.ensemble:
+        return run_ensemble(a)
     st = sp.Stencil2d2h(5, 6, 13) if a.dim == 2 else sp.Stencil3d2h(7, 10, 25)
     cls = MODELS[a.model]
     coeff = a.coeff or ([0.5] if a.model == "C" else [])
@@ -49,6 +55,24 @@ def main(argv=None):
                       "steps": a.steps, "wall_ms_per_step": 1e3 * el / a.steps,
                       "launches": m.launch_count(), "kernel": info}))
     m.close()
+
+
+def run_ensemble(a):
+    members = sp.ensemble_members(a.ensemble, seed=20261203)
+    e = sp.Ensemble(sp.SolverFT(sp.Stencil2d2h(5, 6, 13), form=a.form), members, dtype=a.dtype)
+    for i in range(len(members)):
+        e.fill_uniform(0, 20261203 + i, -0.1, 0.1, inst=i)
+    info = e.autotune(5) if a.autotune else e.kernel_info()
+    e.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        e.step(1)
+    e.synchronize()
+    el = time.perf_counter() - t0
+    print(json.dumps({"ensemble": len(members), "sites": e.sites(), "dtype": a.dtype,
+                      "form": a.form, "steps": a.steps, "wall_ms_per_step": 1e3 * el / a.steps,
+                      "launches": e.launch_count(), "kernel": info}))
+    e.close()
 
 
 if __name__ == "__main__":
