@@ -184,6 +184,21 @@ long long sp_launch_count(const sp_handle* h);
 int sp_field_geometry(const sp_handle* h, int inst, int field, void** dev_origin,
                       long long* pitch, long long* plane, int halo[3]);
 
+/* Structure factor of field `field` of instance `inst`, as SymPhas's SF
+ * collector computes it (dataprocesses/datasf.h:137-245 with the radial
+ * average of datatypes/inc/datalib.h:1120-1330): the interior, thresholded to
+ * 1 where the value is positive and 0 elsewhere when `threshold` is nonzero
+ * (SymPhas's choice) or taken as it is, is Fourier transformed (FP64), and
+ * |F(k)|^2 / (number of sites) is averaged over the classes of wave vectors
+ * whose absolute integer components are equal up to order.  The classes come
+ * in order of radius; k_out[b] is the radius sqrt(i^2 + j^2 + k^2) in units of
+ * the grid's wave-number step (2 pi / (n h) for n points of spacing h) and
+ * s_out[b] the average.  With k_out or s_out null only *nbins is set, to the
+ * number of classes; otherwise *nbins gives the capacity of both arrays and is
+ * set to the number written.  Allocates device scratch; waits for the result. */
+int sp_structure_factor(sp_handle* h, int inst, int field, int threshold, double* k_out,
+                        double* s_out, int* nbins);
+
 /* ---- no-allocation variant of the reduction -------------------------------
  * No counterpart in SymPhas.  For callers that cannot call cudaMalloc -- an
  * application whose device memory belongs to another allocator (a framework's

@@ -100,6 +100,10 @@ SIGNATURES = {
                                                  ctypes.POINTER(ctypes.c_int), ctypes.c_int,
                                                  ctypes.POINTER(ctypes.c_double), ctypes.c_double,
                                                  ctypes.c_int, _P, _P]),
+    "sp_structure_factor": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_double),
+                                           ctypes.POINTER(ctypes.c_double),
+                                           ctypes.POINTER(ctypes.c_int)]),
     "sp_noalloc_error": (ctypes.c_char_p, []),
     "sp_last_error": (ctypes.c_char_p, [_H]),
     "sp_create_error": (ctypes.c_char_p, []),

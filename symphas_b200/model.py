@@ -212,6 +212,19 @@ class Model:
                 self._h)
         return m.value, e.value
 
+    def structure_factor(self, field=0, inst=0, threshold=True):
+        """(k, S): SymPhas's radially averaged structure factor of the field
+        (thresholded at 0 when `threshold`), computed on the device.  k is in
+        units of the wave-number step 2 pi / (n h)."""
+        nb = ctypes.c_int(0)
+        C.check(C.lib().sp_structure_factor(self._h, inst, field, int(bool(threshold)), None,
+                                            None, ctypes.byref(nb)), self._h)
+        k = (ctypes.c_double * nb.value)()
+        sf = (ctypes.c_double * nb.value)()
+        C.check(C.lib().sp_structure_factor(self._h, inst, field, int(bool(threshold)), k, sf,
+                                            ctypes.byref(nb)), self._h)
+        return np.array(k[:nb.value]), np.array(sf[:nb.value])
+
     def autotune(self, reps=20):
         """Pick the fastest tile shape for this kernel and size on this GPU."""
         C.check(C.lib().sp_autotune(self._h, int(reps)), self._h)
