@@ -199,6 +199,29 @@ int sp_field_geometry(const sp_handle* h, int inst, int field, void** dev_origin
 int sp_structure_factor(sp_handle* h, int inst, int field, int threshold, double* k_out,
                         double* s_out, int* nbins);
 
+/* ---- learned jump (surrogate path) ------------------------------------------
+ * No counterpart in SymPhas.  BF16 tensor-core building blocks of the
+ * convolutional surrogate that jumps k steps of the finite-difference solver
+ * at a time; the solver judges every jump.  All pointers are device memory,
+ * activations NHWC bfloat16, work is queued on `stream` (a cudaStream_t). */
+/* z / a [n][h][w][cout] = conv3x3(x [n][h][w][cin], w [cout][3][3][cin]) with
+ * circular padding, + bias (fp32, or null) + res (bf16 NHWC, or null); a gets
+ * gelu(z) (tanh form); either output may be null.  cin a multiple of 32, cout
+ * even. */
+int sp_conv3x3_fwd(const void* x, const void* w, const float* bias, const void* res, void* z,
+                   void* a, int n, int h, int w_, int cin, int cout, void* stream);
+/* dw [cout][3][3][cin] (fp32) += weight gradient of that convolution for the
+ * output gradient dy [n][h][w][cout]; cin a multiple of 32, cout of 8. */
+int sp_conv3x3_wgrad(const void* x, const void* dy, float* dw, int n, int h, int w_, int cin,
+                     int cout, void* stream);
+/* wf [cin][3][3][cout] = w [cout][3][3][cin] rotated by 180 degrees: the input
+ * gradient of the convolution is sp_conv3x3_fwd(dy, wf). */
+int sp_conv3x3_flip(const void* w, void* wf, int cin, int cout, void* stream);
+/* One bias-corrected Adam step (step >= 1) on n fp32 master weights w with
+ * gradient g and moments m, v; writes a bf16 copy to wb when not null. */
+int sp_adam_step(float* w, void* wb, const float* g, float* m, float* v, long long n, float lr,
+                 float b1, float b2, float eps, int step, float weight_decay, void* stream);
+
 /* ---- no-allocation variant of the reduction -------------------------------
  * No counterpart in SymPhas.  For callers that cannot call cudaMalloc -- an
  * application whose device memory belongs to another allocator (a framework's

@@ -104,6 +104,14 @@ SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(ctypes.c_int)]),
+    "sp_conv3x3_fwd": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_int, _P]),
+    "sp_conv3x3_wgrad": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, _P]),
+    "sp_conv3x3_flip": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, _P]),
+    "sp_adam_step": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_longlong, ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                    ctypes.c_float, _P]),
     "sp_noalloc_error": (ctypes.c_char_p, []),
     "sp_last_error": (ctypes.c_char_p, [_H]),
     "sp_create_error": (ctypes.c_char_p, []),

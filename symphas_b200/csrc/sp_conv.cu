@@ -1,0 +1,425 @@
+/*
+ * sp_conv.cu -- the learned jump of the surrogate path: BF16 tensor-core
+ * implicit-GEMM 3x3 convolutions with circular padding (NHWC activations),
+ * their weight gradient, the weight flip that turns the data gradient into a
+ * forward convolution, and the Adam update.  No counterpart in SymPhas; the
+ * finite-difference solver stays the judge of every jump.
+ *
+ * Forward, as a GEMM: rows = pixels (n, y, x), columns = output channels,
+ * K = 9 taps x Cin, tap-major; A[p][t*Cin + c] = x[n, (y+dy) mod H, (x+dx) mod W, c]
+ * is gathered tile by tile (16-byte cp.async, the circular wrap in the
+ * address), B = weights [Cout][9*Cin].  mma.sync m16n8k16 (bf16 in, fp32
+ * accumulate), ldmatrix fragments, two-stage cp.async pipeline.  The epilogue
+ * adds the bias and an optional residual, stores the pre-activation z and,
+ * when asked, gelu(z) (tanh form), both in bf16.
+ */
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/symphas_b200.h"
+
+namespace sp {
+namespace conv {
+
+constexpr int BM = 128, BN = 64, BK = 32, NTH = 128;  // 4 warps: 2 (m) x 2 (n)
+constexpr int SA = BK + 8;                            // padded smem row (bf16): 80 B
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool pred) {
+  const int sz = pred ? 16 : 0;  // zero-fill when out of range
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)),
+               "l"(src), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+__device__ __forceinline__ void ldmatrix_x4(uint32_t (&r)[4], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldmatrix_x2(uint32_t (&r)[2], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n"
+               : "=r"(r[0]), "=r"(r[1])
+               : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4],
+                                         const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+__device__ __forceinline__ float gelu(float z) {
+  const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
+  return 0.5f * z * (1.0f + tanhf(u));
+}
+
+struct FwdParams {
+  const __nv_bfloat16* x;    // [N][H][W][Cin]
+  const __nv_bfloat16* w;    // [Cout][9][Cin]
+  const float* bias;         // [Cout] or null
+  const __nv_bfloat16* res;  // [N][H][W][Cout] added before the activation, or null
+  __nv_bfloat16* z;          // pre-activation out [N][H][W][Cout], or null
+  __nv_bfloat16* a;          // gelu(z) out, or null
+  int n, h, wid, cin, cout;
+};
+
+// one CTA: 128 pixels x 64 output channels
+__global__ void __launch_bounds__(NTH) k_conv3x3_fwd(const FwdParams p) {
+  __shared__ __align__(128) __nv_bfloat16 sa[2][BM][SA];
+  __shared__ __align__(128) __nv_bfloat16 sb[2][BN][SA];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wm = warp >> 1, wn = warp & 1;  // warp tile 64 x 32
+  const long long npix = (long long)p.n * p.h * p.wid;
+  const long long p0 = (long long)blockIdx.x * BM;
+  const int co0 = blockIdx.y * BN;
+  const int kchunks = p.cin / BK;  // per tap
+  const int nk = 9 * kchunks;
+
+  // each thread loads 4 16-byte chunks of A (128 rows x 4 chunks) and 2 of B
+  // (64 rows x 4 chunks) per K step; the pixel coordinates of its A rows
+  int arow[4], ay[4], ax[4];
+  long long abase[4];
+  bool aok[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = (tid + i * NTH) >> 2;
+    arow[i] = r;
+    const long long pix = p0 + r;
+    aok[i] = pix < npix;
+    const long long pp = aok[i] ? pix : 0;
+    const int xx = int(pp % p.wid);
+    const int yy = int((pp / p.wid) % p.h);
+    const long long nn = pp / ((long long)p.wid * p.h);
+    ax[i] = xx;
+    ay[i] = yy;
+    abase[i] = nn * p.h * p.wid;
+  }
+  auto load = [&](int stage, int kstep) {
+    const int tap = kstep / kchunks, c0 = (kstep % kchunks) * BK;
+    const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int chunk = (tid + i * NTH) & 3;
+      int yy = ay[i] + dy, xx = ax[i] + dx;
+      yy += (yy < 0) ? p.h : 0;
+      yy -= (yy >= p.h) ? p.h : 0;
+      xx += (xx < 0) ? p.wid : 0;
+      xx -= (xx >= p.wid) ? p.wid : 0;
+      const __nv_bfloat16* src =
+          p.x + ((abase[i] + (long long)yy * p.wid + xx) * p.cin + c0 + chunk * 8);
+      cp_async16(&sa[stage][arow[i]][chunk * 8], src, aok[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int r = (tid + i * NTH) >> 2, chunk = (tid + i * NTH) & 3;
+      const int co = co0 + r;
+      const bool ok = co < p.cout;
+      const __nv_bfloat16* src = p.w + ((long long)(ok ? co : 0) * 9 * p.cin + tap * p.cin + c0 +
+                                        chunk * 8);
+      cp_async16(&sb[stage][r][chunk * 8], src, ok);
+    }
+    cp_async_commit();
+  };
+
+  float acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[i][j][k] = 0.f;
+
+  load(0, 0);
+  for (int ks = 0; ks < nk; ++ks) {
+    const int st = ks & 1;
+    if (ks + 1 < nk) {
+      load(st ^ 1, ks + 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 16) {
+      uint32_t af[4][4], bf[4][2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = wm * 64 + i * 16 + (lane & 15);
+        const int c = kk + (lane >> 4) * 8;
+        ldmatrix_x4(af[i], &sa[st][r][c]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int r = wn * 32 + j * 8 + (lane & 7);
+        const int c = kk + ((lane >> 3) & 1) * 8;
+        ldmatrix_x2(bf[j], &sb[st][r][c]);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) mma16816(acc[i][j], af[i], bf[j]);
+    }
+    __syncthreads();
+  }
+
+  // epilogue: fragment element e of tile (i, j) is row wm*64 + i*16 + lane/4
+  // (+8 for e >= 2), column wn*32 + j*8 + (lane%4)*2 (+1 for odd e)
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const long long pix = p0 + wm * 64 + i * 16 + (lane >> 2) + half * 8;
+      if (pix >= npix) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int co = co0 + wn * 32 + j * 8 + (lane & 3) * 2;
+        if (co >= p.cout) continue;
+        float v0 = acc[i][j][half * 2], v1 = acc[i][j][half * 2 + 1];
+        if (p.bias) {
+          v0 += p.bias[co];
+          v1 += p.bias[co + 1];
+        }
+        const long long o = pix * p.cout + co;
+        if (p.res) {
+          const __nv_bfloat162 r = *reinterpret_cast<const __nv_bfloat162*>(p.res + o);
+          v0 += __bfloat162float(r.x);
+          v1 += __bfloat162float(r.y);
+        }
+        if (p.z) *reinterpret_cast<__nv_bfloat162*>(p.z + o) = __floats2bfloat162_rn(v0, v1);
+        if (p.a)
+          *reinterpret_cast<__nv_bfloat162*>(p.a + o) = __floats2bfloat162_rn(gelu(v0), gelu(v1));
+      }
+    }
+}
+
+}  // namespace conv
+}  // namespace sp
+
+namespace sp {
+namespace conv {
+
+__device__ __forceinline__ void ldmatrix_x4_t(uint32_t (&r)[4], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldmatrix_x2_t(uint32_t (&r)[2], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n"
+               : "=r"(r[0]), "=r"(r[1])
+               : "r"(smem_u32(p)));
+}
+
+// Weight gradient dw[co][t][c] += sum over pixels p of dy[p][co] * x[p + d_t][c],
+// as a GEMM with rows (t, c) (a 32-channel block of one tap per CTA), columns
+// co (64 per CTA) and K = pixels; each CTA sums `chunk` pixels and adds its
+// fp32 tile into dw with atomics (split K).  Both operands are stored with
+// the pixel (K) index outer, so their fragments come from ldmatrix.trans.
+constexpr int WM = 32, WN = 64, WK = 32, WTH = 128;  // 4 warps along columns
+constexpr int WSX = WM + 8, WSD = WN + 8;             // padded smem rows (bf16)
+
+struct WgradParams {
+  const __nv_bfloat16* x;   // [N][H][W][Cin]
+  const __nv_bfloat16* dy;  // [N][H][W][Cout]
+  float* dw;                // [Cout][9][Cin], accumulated
+  int n, h, wid, cin, cout;
+  long long chunk;          // pixels per CTA (multiple of WK)
+};
+
+__global__ void __launch_bounds__(WTH) k_conv3x3_wgrad(const WgradParams p) {
+  __shared__ __align__(128) __nv_bfloat16 sx[2][WK][WSX];
+  __shared__ __align__(128) __nv_bfloat16 sd[2][WK][WSD];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cblocks = p.cin / WM;
+  const int tap = blockIdx.x / cblocks, c0 = (blockIdx.x % cblocks) * WM;
+  const int dy_ = tap / 3 - 1, dx_ = tap % 3 - 1;
+  const int co0 = blockIdx.y * WN;
+  const long long npix = (long long)p.n * p.h * p.wid;
+  const long long pb = (long long)blockIdx.z * p.chunk;
+  const long long pe = pb + p.chunk < npix ? pb + p.chunk : npix;
+  if (pb >= pe) return;
+  const int nk = int((pe - pb + WK - 1) / WK);
+
+  auto load = [&](int st, int ks) {
+    const long long q0 = pb + (long long)ks * WK;
+    {  // x: 32 pixels x 32 channels = 128 chunks of 16 B, one per thread
+      const int r = tid >> 2, ch = tid & 3;
+      const long long pix = q0 + r;
+      const bool ok = pix < pe;
+      const long long pp = ok ? pix : pb;
+      const int xx0 = int(pp % p.wid), yy0 = int((pp / p.wid) % p.h);
+      const long long nn = pp / ((long long)p.wid * p.h);
+      int yy = yy0 + dy_, xx = xx0 + dx_;
+      yy += (yy < 0) ? p.h : 0;
+      yy -= (yy >= p.h) ? p.h : 0;
+      xx += (xx < 0) ? p.wid : 0;
+      xx -= (xx >= p.wid) ? p.wid : 0;
+      const __nv_bfloat16* src = p.x + (((nn * p.h + yy) * p.wid + xx) * p.cin + c0 + ch * 8);
+      cp_async16(&sx[st][r][ch * 8], src, ok);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {  // dy: 32 pixels x 64 channels = 256 chunks
+      const int idx = tid + i * WTH, r = idx >> 3, ch = idx & 7;
+      const long long pix = q0 + r;
+      const int co = co0 + ch * 8;
+      const bool ok = pix < pe && co < p.cout;
+      const __nv_bfloat16* src = p.dy + ((ok ? pix : pb) * p.cout + (ok ? co : 0));
+      cp_async16(&sd[st][r][ch * 8], src, ok);
+    }
+    cp_async_commit();
+  };
+
+  float acc[2][2][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[i][j][k] = 0.f;
+
+  load(0, 0);
+  for (int ks = 0; ks < nk; ++ks) {
+    const int st = ks & 1;
+    if (ks + 1 < nk) {
+      load(st ^ 1, ks + 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < WK; kk += 16) {
+      uint32_t af[2][4], bf[2][2];
+      const int q = lane >> 3;
+#pragma unroll
+      for (int i = 0; i < 2; ++i)  // rows (channels) i*16 .. +15
+        ldmatrix_x4_t(af[i], &sx[st][kk + (lane & 7) + (q >> 1) * 8][i * 16 + (q & 1) * 8]);
+#pragma unroll
+      for (int j = 0; j < 2; ++j)  // columns warp*16 + j*8 .. +7
+        ldmatrix_x2_t(bf[j], &sd[st][kk + (lane & 7) + ((lane >> 3) & 1) * 8][warp * 16 + j * 8]);
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) mma16816(acc[i][j], af[i], bf[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const int c = c0 + i * 16 + (lane >> 2) + half * 8;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int co = co0 + warp * 16 + j * 8 + (lane & 3) * 2;
+        if (co >= p.cout) continue;
+        float* d = p.dw + ((long long)co * 9 + tap) * p.cin + c;
+        atomicAdd(d, acc[i][j][half * 2]);
+        atomicAdd(d + 9LL * p.cin, acc[i][j][half * 2 + 1]);
+      }
+    }
+}
+
+// wf[c][t][co] = w[co][8 - t][c]: the forward weights of the data gradient
+__global__ void k_conv3x3_flip(const __nv_bfloat16* w, __nv_bfloat16* wf, int cin, int cout) {
+  const long long total = 9LL * cin * cout;
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+       id += (long long)gridDim.x * blockDim.x) {
+    const int co = int(id % cout), t = int((id / cout) % 9);
+    const long long c = id / (9LL * cout);
+    wf[(c * 9 + t) * cout + co] = w[((long long)co * 9 + (8 - t)) * cin + c];
+  }
+}
+
+// Adam (bias-corrected), fp32 master weights, bf16 copy for the convolutions
+__global__ void k_adam(float* w, __nv_bfloat16* wb, const float* g, float* m, float* v,
+                       long long n, float lr, float b1, float b2, float eps, float c1, float c2,
+                       float wd) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float gi = g[i] + wd * w[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16_rn(wi);
+  }
+}
+
+int sms() {
+  static int n = [] {
+    int dev = 0, v = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v;
+  }();
+  return n;
+}
+
+}  // namespace conv
+}  // namespace sp
+
+extern "C" {
+
+int sp_conv3x3_fwd(const void* x, const void* w, const float* bias, const void* res, void* z,
+                   void* a, int n, int h, int w_, int cin, int cout, void* stream) {
+  using namespace sp::conv;
+  if (!x || !w || (!z && !a) || n < 1 || h < 1 || w_ < 1 || cin % BK != 0 || cout % 2 != 0 ||
+      cout < 2)
+    return SP_EINVAL;
+  FwdParams p{static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w), bias,
+              static_cast<const __nv_bfloat16*>(res), static_cast<__nv_bfloat16*>(z),
+              static_cast<__nv_bfloat16*>(a), n, h, w_, cin, cout};
+  const long long npix = (long long)n * h * w_;
+  dim3 grid(unsigned((npix + BM - 1) / BM), unsigned((cout + BN - 1) / BN));
+  k_conv3x3_fwd<<<grid, NTH, 0, static_cast<cudaStream_t>(stream)>>>(p);
+  return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ECUDA;
+}
+
+int sp_conv3x3_wgrad(const void* x, const void* dy, float* dw, int n, int h, int w_, int cin,
+                     int cout, void* stream) {
+  using namespace sp::conv;
+  if (!x || !dy || !dw || n < 1 || h < 1 || w_ < 1 || cin % WM != 0 || cout % 8 != 0)
+    return SP_EINVAL;
+  const long long npix = (long long)n * h * w_;
+  const unsigned gx = unsigned(9 * (cin / WM)), gy = unsigned((cout + WN - 1) / WN);
+  // enough pixel chunks for about four waves of CTAs
+  long long want = (long long)sms() * 8 / (gx * gy);
+  if (want < 1) want = 1;
+  long long chunk = (npix + want - 1) / want;
+  chunk = ((chunk + WK - 1) / WK) * WK;
+  if (chunk < 1024) chunk = 1024;
+  const unsigned gz = unsigned((npix + chunk - 1) / chunk);
+  WgradParams p{static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy), dw,
+                n, h, w_, cin, cout, chunk};
+  k_conv3x3_wgrad<<<dim3(gx, gy, gz), WTH, 0, static_cast<cudaStream_t>(stream)>>>(p);
+  return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ECUDA;
+}
+
+int sp_conv3x3_flip(const void* w, void* wf, int cin, int cout, void* stream) {
+  if (!w || !wf || cin < 1 || cout < 1) return SP_EINVAL;
+  sp::conv::k_conv3x3_flip<<<256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const __nv_bfloat16*>(w), static_cast<__nv_bfloat16*>(wf), cin, cout);
+  return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ECUDA;
+}
+
+int sp_adam_step(float* w, void* wb, const float* g, float* m, float* v, long long n, float lr,
+                 float b1, float b2, float eps, int step, float weight_decay, void* stream) {
+  if (!w || !g || !m || !v || n < 1 || step < 1) return SP_EINVAL;
+  const float c1 = 1.f - powf(b1, float(step)), c2 = 1.f - powf(b2, float(step));
+  const int blocks = int((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024);
+  sp::conv::k_adam<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      w, static_cast<__nv_bfloat16*>(wb), g, m, v, n, lr, b1, b2, eps, c1, c2, weight_decay);
+  return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ECUDA;
+}
+
+}  // extern "C"
