@@ -162,6 +162,18 @@ class Model:
         C.check(C.lib().sp_download(self._h, inst, field, ctypes.c_void_p(host_ptr), nbytes),
                 self._h)
 
+    def field_to_device(self, field, dev_ptr, nbytes, inst=0):
+        """Copy the interior to device memory (compact, x fastest), in the
+        order of the handle's stream (no host wait)."""
+        C.check(C.lib().sp_download_device(self._h, inst, field, ctypes.c_void_p(dev_ptr),
+                                           nbytes), self._h)
+
+    def field_from_device(self, field, dev_ptr, nbytes, inst=0):
+        """Set the interior from device memory (compact, x fastest) and refresh
+        the halo, in the order of the handle's stream."""
+        C.check(C.lib().sp_upload_device(self._h, inst, field, ctypes.c_void_p(dev_ptr),
+                                         nbytes), self._h)
+
     def fill_uniform(self, field, seed, lo, hi, inst=0):
         """Seeded SplitMix64 initial values, bit-identical to the oracle."""
         C.check(C.lib().sp_fill_uniform(self._h, inst, field, seed, lo, hi), self._h)
