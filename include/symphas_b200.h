@@ -139,6 +139,16 @@ int sp_fill_uniform(sp_handle* h, int inst, int field, uint64_t seed, double lo,
 /* Advance every instance by `nsteps` forward-Euler iterations. */
 int sp_step(sp_handle* h, int nsteps);
 
+/* Keep the mass of field 0 of every instance at its present value: from now
+ * on, after every `every` steps, sp_step reduces each instance's mass in FP64
+ * and shifts the field uniformly (interior and periodic halo) so the mass
+ * returns to the value it had at this call; every = 0 turns it off.  For
+ * conserved fields (models B, BMK, field psi of C) in FP32, whose stored
+ * values round at every step; all queued on the handle's stream, no host
+ * wait.  Needs periodic boundaries on every axis.  No counterpart in SymPhas,
+ * whose FP64 steps need none. */
+int sp_conserve_mass(sp_handle* h, int every);
+
 /* Advance every instance by `nsteps` (>= 1) iterations; the last one also sums
  * field 0 of each instance in FP64 inside the step kernel (warp shuffles) and
  * writes the `batch` sums to `mass`.  Waits for the result. */

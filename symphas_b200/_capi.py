@@ -112,6 +112,7 @@ SIGNATURES = {
     "sp_adam_step": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_longlong, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int,
                                     ctypes.c_float, _P]),
+    "sp_conserve_mass": (ctypes.c_int, [_H, ctypes.c_int]),
     "sp_noalloc_error": (ctypes.c_char_p, []),
     "sp_last_error": (ctypes.c_char_p, [_H]),
     "sp_create_error": (ctypes.c_char_p, []),

@@ -225,8 +225,9 @@ int fill_halo_t(sp_handle* H, int which, int inst, int f) {
     p.bc[s] = H->d.boundary[s];
     p.bv[s] = T(H->d.boundary_value[s]);
   }
-  const long long cells = (g.n[0] + 2LL * H->h[0]) * (g.n[1] + 2LL * H->h[1]) *
-                          (H->dim == 3 ? g.n[2] + 2LL * H->h[2] : 1);
+  const long long L0 = g.n[0] + 2LL * H->h[0], L1 = g.n[1] + 2LL * H->h[1];
+  const long long n2 = H->dim == 3 ? g.n[2] : 1, h2 = H->dim == 3 ? H->h[2] : 0;
+  const long long cells = 2 * h2 * L0 * L1 + n2 * 2 * H->h[1] * L0 + n2 * g.n[1] * 2 * H->h[0];
   const int blocks = int(std::min<long long>(H->sms * 4LL, (cells + 255) / 256));
   sp::k_fill_halo<T><<<blocks, 256, 0, H->stream>>>(p);
   SP_CUDA(H, cudaGetLastError());
@@ -279,6 +280,8 @@ void release(sp_handle* H) {
   cudaFree(H->partial_d);
   cudaFree(H->result_d);
   cudaFree(H->err_d);
+  cudaFree(H->mass_target_d);
+  cudaFree(H->cons_d);
   if (H->result_h) cudaFreeHost(H->result_h);
   if (H->own_stream && H->stream) cudaStreamDestroy(H->stream);
   delete H;
@@ -647,8 +650,9 @@ int capture_graph(sp_handle* H) {
   return SP_OK;
 }
 
+// queue the FP64 (mass, energy) reduction of a field into out[0..1] (device)
 template <class T>
-int reduce_t(sp_handle* H, int inst, int field, double* mass, double* energy) {
+int enqueue_reduce_t(sp_handle* H, int inst, int field, double* out) {
   const InstGeo& g = H->geo[inst];
   sp::ReduceParams<T> p{};
   p.f0 = reinterpret_cast<const T*>(field_base(H, H->cur, inst, field));
@@ -674,8 +678,51 @@ int reduce_t(sp_handle* H, int inst, int field, double* mass, double* energy) {
   blocks = std::max(blocks, 1);
   sp::k_reduce<T, RED_THREADS><<<blocks, RED_THREADS, 0, H->stream>>>(p);
   SP_CUDA(H, cudaGetLastError());
-  sp::k_finish<RED_THREADS><<<1, RED_THREADS, 0, H->stream>>>(H->partial_d, blocks, 2, H->result_d);
+  sp::k_finish<RED_THREADS><<<1, RED_THREADS, 0, H->stream>>>(H->partial_d, blocks, 2, out);
   SP_CUDA(H, cudaGetLastError());
+  return SP_OK;
+}
+
+int enqueue_reduce(sp_handle* H, int inst, int field, double* out) {
+  return H->esz == 4 ? enqueue_reduce_t<float>(H, inst, field, out)
+                     : enqueue_reduce_t<double>(H, inst, field, out);
+}
+
+// restore the mass of field 0 of every instance to its target (no host wait)
+int conserve_pass(sp_handle* H) {
+  for (int i = 0; i < H->batch; ++i) {
+    if (int rc = enqueue_reduce(H, i, 0, H->cons_d)) return rc;
+    const InstGeo& g = H->geo[i];
+    sp::ShiftParams sh{};
+    sh.dim = H->dim;
+    for (int a = 0; a < 3; ++a) {
+      sh.n[a] = g.n[a];
+      sh.h[a] = H->h[a];
+    }
+    sh.pitch = g.pitch;
+    sh.plane = g.plane;
+    sh.pass = ++H->conserve_passes;
+    const long long cells = (g.n[0] + 2LL * H->h[0]) * (g.n[1] + 2LL * H->h[1]) *
+                            (H->dim == 3 ? g.n[2] + 2LL * H->h[2] : 1);
+    const int blocks = int(std::min<long long>(H->sms * 8LL, (cells + 255) / 256));
+    if (H->esz == 4)
+      sp::k_mass_shift<float><<<blocks, 256, 0, H->stream>>>(
+          reinterpret_cast<float*>(field_base(H, H->cur, i, 0)), sh, H->cons_d,
+          H->mass_target_d + 2 * i, double(g.sites()));
+    else
+      sp::k_mass_shift<double><<<blocks, 256, 0, H->stream>>>(
+          reinterpret_cast<double*>(field_base(H, H->cur, i, 0)), sh, H->cons_d,
+          H->mass_target_d + 2 * i, double(g.sites()));
+    SP_CUDA(H, cudaGetLastError());
+  }
+  return SP_OK;
+}
+
+// sp_step without mass conservation: graph-replayed chunks, then single launches
+int step_plain(sp_handle* H, int nsteps);
+
+int reduce(sp_handle* H, int inst, int field, double* mass, double* energy) {
+  if (int rc = enqueue_reduce(H, inst, field, H->result_d)) return rc;
   SP_CUDA(H, cudaMemcpyAsync(H->result_h, H->result_d, 2 * sizeof(double),
                              cudaMemcpyDeviceToHost, H->stream));
   if (int rc = check_err_flag(H)) return rc;
@@ -747,6 +794,42 @@ int sp_fill_uniform(sp_handle* H, int inst, int field, uint64_t seed, double lo,
 
 int sp_step(sp_handle* H, int nsteps) {
   if (!H || nsteps < 0) return SP_EINVAL;
+  if (H->conserve_every <= 0) return step_plain(H, nsteps);
+  // a pass falls due after every conserve_every steps (sp_step_mass counts too)
+  do {
+    if (H->since_conserve >= H->conserve_every) {
+      if (int rc = conserve_pass(H)) return rc;
+      H->since_conserve = 0;
+    }
+    const int k = std::min(nsteps, H->conserve_every - H->since_conserve);
+    if (int rc = step_plain(H, k)) return rc;
+    nsteps -= k;
+    H->since_conserve += k;
+  } while (nsteps > 0 || H->since_conserve >= H->conserve_every);
+  return SP_OK;
+}
+
+int sp_conserve_mass(sp_handle* H, int every) {
+  if (!H || every < 0) return SP_EINVAL;
+  if (every > 0) {
+    for (int a = 0; a < H->dim; ++a)
+      if (H->d.boundary[2 * a] != SP_PERIODIC)
+        return fail(H, SP_EINVAL, "mass conservation needs periodic boundaries on every axis");
+    if (!H->mass_target_d) SP_CUDA(H, cudaMalloc(&H->mass_target_d, 2 * sizeof(double) * H->batch));
+    if (!H->cons_d) SP_CUDA(H, cudaMalloc(&H->cons_d, 2 * sizeof(double)));
+    for (int i = 0; i < H->batch; ++i)
+      if (int rc = enqueue_reduce(H, i, 0, H->mass_target_d + 2 * i)) return rc;
+    if (int rc = check_err_flag(H)) return rc;
+  }
+  H->conserve_every = every;
+  H->since_conserve = 0;
+  return SP_OK;
+}
+
+}  // extern "C"
+
+namespace {
+int step_plain(sp_handle* H, int nsteps) {
   while (nsteps > 0) {
     if (nsteps >= GRAPH_STEPS && H->graphs && !H->gexec[H->cur])
       if (int rc = capture_graph(H)) return rc;
@@ -761,6 +844,9 @@ int sp_step(sp_handle* H, int nsteps) {
   }
   return SP_OK;
 }
+}  // namespace
+
+extern "C" {
 
 int sp_step_mass(sp_handle* H, int nsteps, double* mass) {
   if (!H || nsteps < 1 || !mass) return SP_EINVAL;
@@ -768,6 +854,7 @@ int sp_step_mass(sp_handle* H, int nsteps, double* mass) {
     return fail(H, SP_EINVAL, "fused mass reduction needs dim 3 or a single 2D instance");
   if (int rc = sp_step(H, nsteps - 1)) return rc;
   if (int rc = launch_step(H, 0, H->partial_d)) return rc;
+  if (H->conserve_every > 0) ++H->since_conserve;  // its pass runs before the next step
   const int per = H->dim == 3 ? H->ntx * H->nty * H->nzc : H->grid2;
   for (int i = 0; i < H->batch; ++i) {
     sp::k_finish<RED_THREADS><<<1, RED_THREADS, 0, H->stream>>>(H->partial_d + size_t(i) * per,
@@ -802,8 +889,7 @@ int sp_reduce(sp_handle* H, int inst, int field, double* mass, double* energy) {
   if (!H) return SP_EINVAL;
   if (inst < 0 || inst >= H->batch || field < 0 || field >= H->nf)
     return fail(H, SP_EINVAL, "instance or field index out of range");
-  return H->esz == 4 ? reduce_t<float>(H, inst, field, mass, energy)
-                     : reduce_t<double>(H, inst, field, mass, energy);
+  return reduce(H, inst, field, mass, energy);
 }
 
 int sp_autotune(sp_handle* H, int reps) {

@@ -25,19 +25,38 @@ struct HaloParams {
   T bv[6];
 };
 
+// The halo cells only, enumerated as (a) the whole halo planes in z, (b) the
+// whole halo rows in y of the interior planes, (c) the halo columns in x of
+// the interior rows.
 template <class T>
 __global__ void k_fill_halo(const HaloParams<T> p) {
   const long long L0 = p.n[0] + 2 * p.h[0], L1 = p.n[1] + 2 * p.h[1];
-  const long long L2 = (p.dim == 3) ? p.n[2] + 2 * p.h[2] : 1;
-  const long long total = L0 * L1 * L2;
+  const int n2 = (p.dim == 3) ? p.n[2] : 1, h2 = (p.dim == 3) ? p.h[2] : 0;
+  const long long A = 2LL * h2 * L0 * L1;            // halo planes
+  const long long B = (long long)n2 * 2 * p.h[1] * L0;  // halo rows of interior planes
+  const long long Cc = (long long)n2 * p.n[1] * 2 * p.h[0];  // halo columns
+  const long long total = A + B + Cc;
   for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
        id += (long long)gridDim.x * blockDim.x) {
-    const long long i = id % L0, j = (id / L0) % L1, k = id / (L0 * L1);
+    long long i, j, k;  // padded coordinates
+    if (id < A) {
+      const long long q = id / (L0 * L1), r = id % (L0 * L1);
+      k = q < h2 ? q : n2 + q;
+      j = r / L0;
+      i = r % L0;
+    } else if (id < A + B) {
+      const long long e = id - A, q = e / L0;
+      i = e % L0;
+      const long long row = q % (2 * p.h[1]);
+      k = h2 + q / (2 * p.h[1]);
+      j = row < p.h[1] ? row : p.n[1] + row;
+    } else {
+      const long long e = id - A - B, col = e % (2 * p.h[0]), q = e / (2 * p.h[0]);
+      i = col < p.h[0] ? col : p.n[0] + col;
+      j = p.h[1] + q % p.n[1];
+      k = h2 + q / p.n[1];
+    }
     long long c[3] = {i - p.h[0], j - p.h[1], (p.dim == 3) ? k - p.h[2] : 0};
-    bool outside = false;
-    for (int a = 0; a < p.dim; ++a)
-      if (c[a] < 0 || c[a] >= p.n[a]) outside = true;
-    if (!outside) continue;
     int dir = -1;
     T dval = T(0);
     for (int a = 0; a < p.dim; ++a) {
@@ -136,6 +155,61 @@ __global__ void __launch_bounds__(NT)
     const double t = block_sum<NT>(v, red);
     if (threadIdx.x == 0) out[s] = t;
     __syncthreads();
+  }
+}
+
+// Mass-restoring shift of one field: every cell of the padded box, interior
+// and halo, becomes value + s with s = (target - mass) / sites.  In FP32 a
+// shift far below one ulp would round away at nearly every cell, so the sum
+// is rounded stochastically instead: each cell takes the float just below or
+// just above value + s with the probabilities that make its expectation
+// value + s exactly (the restored mass is then within about sqrt(|N s| ulp) of
+// the target).  The uniform draw hashes the interior site a cell shows (its
+// periodic source for a halo cell) and the pass number, so a halo image
+// rounds exactly like its source.  FP64 adds s.
+struct ShiftParams {
+  int dim;
+  int n[3], h[3];
+  long long pitch, plane;
+  unsigned long long pass;
+};
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+template <class T>
+__global__ void k_mass_shift(T* base, const ShiftParams p, const double* mass,
+                             const double* target, double sites) {
+  const double s = (*target - *mass) / sites;
+  const long long L0 = p.n[0] + 2 * p.h[0], L1 = p.n[1] + 2 * p.h[1];
+  const long long L2 = (p.dim == 3) ? p.n[2] + 2 * p.h[2] : 1;
+  const long long total = L0 * L1 * L2;
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+       id += (long long)gridDim.x * blockDim.x) {
+    const long long i = id % L0, j = (id / L0) % L1, k = id / (L0 * L1);
+    T& cell = base[k * p.plane + j * p.pitch + i];
+    if constexpr (sizeof(T) == 8) {
+      cell += s;
+    } else {
+      long long c[3] = {i - p.h[0], j - p.h[1], (p.dim == 3) ? k - p.h[2] : 0};
+      for (int a = 0; a < p.dim; ++a) {
+        c[a] %= p.n[a];
+        if (c[a] < 0) c[a] += p.n[a];
+      }
+      const unsigned long long key =
+          (unsigned long long)((c[2] * p.n[1] + c[1]) * p.n[0] + c[0]);
+      const double v = double(cell) + s;
+      const float f = float(v);
+      const float lo = double(f) > v ? nextafterf(f, -INFINITY) : f;
+      const float hi = double(f) > v ? f : nextafterf(f, INFINITY);
+      const double frac = (v - double(lo)) / (double(hi) - double(lo));
+      const double u = double(mix64(key * 0x9E3779B97F4A7C15ULL ^ (p.pass << 1)) >> 11) *
+                       (1.0 / 9007199254740992.0);
+      cell = T(u < frac ? hi : lo);
+    }
   }
 }
 

@@ -67,6 +67,13 @@ struct sp_handle {
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   bool graphs = true;  // false once capture failed on this stream
   long long launches = 0;
+  // mass conservation of field 0 (sp_conserve_mass): every `conserve_every`
+  // steps, restore each instance's mass to its target (2 doubles per instance:
+  // the target mass and the energy reduced alongside it)
+  int conserve_every = 0, since_conserve = 0;
+  unsigned long long conserve_passes = 0;  // seeds the stochastic rounding
+  double* mass_target_d = nullptr;
+  double* cons_d = nullptr;  // [2] the latest reduction
   std::string err;
 };
 

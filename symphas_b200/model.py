@@ -216,6 +216,11 @@ class Model:
         self.time += n * dt
         return np.array(out[:])
 
+    def conserve_mass(self, every=100):
+        """From now on restore the FP64 mass of field 0 every `every` steps
+        (uniform shift; 0 turns it off)."""
+        C.check(C.lib().sp_conserve_mass(self._h, int(every)), self._h)
+
     def reduce(self, field=0, inst=0):
         """(mass, free energy) in FP64."""
         m = ctypes.c_double()

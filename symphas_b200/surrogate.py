@@ -404,6 +404,8 @@ def main(argv=None):
     ap.add_argument("--nsnap", type=int, default=60, help="jumps per trajectory")
     ap.add_argument("--jump", type=int, default=100, help="FD steps per jump")
     ap.add_argument("--dt", type=float, default=0.01)
+    ap.add_argument("--warm", type=int, default=0,
+                    help="FD steps before the first snapshot (training and evaluation)")
     ap.add_argument("--steps", type=int, default=2000, help="optimiser steps")
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--lr", type=float, default=1e-3)
@@ -418,12 +420,12 @@ def main(argv=None):
     torch.cuda.set_device(0)
     net = JumpNet(tuple(a.channels))
     report = {"params": net.nparams(), "channels": list(a.channels), "n": a.n, "jump": a.jump,
-              "dt": a.dt}
+              "dt": a.dt, "warm": a.warm, "flops_per_sample": net.flops(a.n)}
     if a.load:
         net.load(torch.load(a.load))
     else:
         t0 = time.perf_counter()
-        snaps = trajectories(a.ntraj, a.nsnap, a.jump, a.n, a.dt, seed=1)
+        snaps = trajectories(a.ntraj, a.nsnap, a.jump, a.n, a.dt, seed=1, warm=a.warm)
         report["data_s"] = time.perf_counter() - t0
         report["pairs"] = a.ntraj * a.nsnap
         t0 = time.perf_counter()
@@ -435,7 +437,7 @@ def main(argv=None):
         if a.save:
             torch.save(net.state(), a.save)
     report["eval"] = evaluate(net, a.eval_batch, a.eval_jumps, a.jump, a.judge_steps, a.dt,
-                              n=a.n, threshold=a.threshold)
+                              warm=a.warm, n=a.n, threshold=a.threshold)
     print(json.dumps(report))
 
 
