@@ -231,6 +231,7 @@ __global__ void __launch_bounds__(TC::NT)
                      (!p.per[0] || (x0 >= R && x0 + TX <= p.n[0] - R)) &&
                      (!p.per[1] || (y0 >= R && y0 + TY <= p.n[1] - R));
   const bool ragged = xin && !vec_ok;
+  const bool xany = p.per[0] && (x0 < R || x0 + TX + W > p.n[0] - R);
   const bool do_mass = p.partial != nullptr;
   // the mu cell beyond this thread's own ones, if any: own cells are stage
   // rows RS..TY+RS-1 and column groups RSA/W..RSA/W+TXT-1; the ring is the
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(TC::NT)
       } else {
 #pragma unroll
         for (int k = 0; k < SPT; ++k) {
-          put_images_pred(orow[k] + zoff, nv[k], rowin[k] && vec_ok, xo, yo[k], zo);
+          put_images_pred(orow[k] + zoff, nv[k], rowin[k] && vec_ok, xany, xo, yo[k], zo);
           if (ragged && rowin[k])
             store_group<T, W, 3, R>(p.out[blockIdx.z], x, y0 + row0 + k, zi, nv[k], p.n, p.h,
                                     p.per, p.pitch, p.plane);

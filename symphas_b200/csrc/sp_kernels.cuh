@@ -202,20 +202,28 @@ __device__ __forceinline__ void st_if(T* p, const V& v, bool on) {
 }
 
 // A whole W-group at b (padded address of an interior site) and its periodic
-// images (offsets xo, yo, zo; 0 where there is none), all predicated; `in`
-// says whether the group exists.  zo is uniform across the block (one plane).
+// images (offsets xo, yo, zo; 0 where there is none); `in` says whether the
+// group exists.  xany: some lane of the block has an x image (block-uniform);
+// yo is uniform across a warp (a warp holds whole rows) and zo across the
+// block (one plane), so only the x images are predicated per lane and the
+// other cases are uniform branches.
 template <class T, class V>
-__device__ __forceinline__ void put_images_pred(T* b, const V& v, bool in, long long xo,
-                                                long long yo, long long zo) {
+__device__ __forceinline__ void put_images_pred(T* b, const V& v, bool in, bool xany,
+                                                long long xo, long long yo, long long zo) {
+  const bool xi = in && xo != 0;
   st_if(b, v, in);
-  st_if(b + xo, v, in && xo != 0);
-  st_if(b + yo, v, in && yo != 0);
-  st_if(b + xo + yo, v, in && xo != 0 && yo != 0);
+  if (xany) st_if(b + xo, v, xi);
+  if (yo != 0) {
+    st_if(b + yo, v, in);
+    if (xany) st_if(b + xo + yo, v, xi);
+  }
   if (zo != 0) {
     st_if(b + zo, v, in);
-    st_if(b + zo + xo, v, in && xo != 0);
-    st_if(b + zo + yo, v, in && yo != 0);
-    st_if(b + zo + xo + yo, v, in && xo != 0 && yo != 0);
+    if (xany) st_if(b + zo + xo, v, xi);
+    if (yo != 0) {
+      st_if(b + zo + yo, v, in);
+      if (xany) st_if(b + zo + xo + yo, v, xi);
+    }
   }
 }
 
@@ -378,6 +386,8 @@ __global__ void __launch_bounds__(TC::NT)
                      (!p.per[0] || (x0 >= R && x0 + TX <= p.n[0] - R)) &&
                      (!p.per[1] || (y0 >= R && y0 + TY <= p.n[1] - R));
   const bool ragged = xin && !vec_ok;  // a group cut by the end of the row
+  // some thread of the block has an x image (the same for every thread)
+  const bool xany = p.per[0] && (x0 < R || x0 + TX + W > p.n[0] - R);
   const bool do_mass = p.partial != nullptr;
   // the stage cells beyond this thread's row groups, if any
   int xsr[NX1], xsc[NX1];
@@ -537,7 +547,7 @@ __global__ void __launch_bounds__(TC::NT)
         for (int k = 0; k < SPT; ++k) {
 #pragma unroll
           for (int f = 0; f < NF; ++f)
-            put_images_pred(orow[k][f] + zoff, nv[k][f], rowin[k] && vec_ok, xo, yo[k], zo);
+            put_images_pred(orow[k][f] + zoff, nv[k][f], rowin[k] && vec_ok, xany, xo, yo[k], zo);
           if (ragged && rowin[k]) {
 #pragma unroll
             for (int f = 0; f < NF; ++f)
@@ -758,6 +768,7 @@ __device__ __forceinline__ void fd2_out(const Step2Params<T>& p, const M& m, con
     // images as predicated stores (no divergence); a group cut by the end of
     // a row element by element
     const bool ragged = x < n0 && !vec_ok;
+    const bool xany = ip.per[0] && (x0 < R || x0 + TX + W > n0 - R);
 #pragma unroll
     for (int k = 0; k < SPT; ++k) {
       const int y = y0 + row0 + k;
@@ -766,7 +777,7 @@ __device__ __forceinline__ void fd2_out(const Step2Params<T>& p, const M& m, con
 #pragma unroll
       for (int f = 0; f < NF; ++f)
         put_images_pred(out[f] + (long long)(y + p.hy) * pitch + x + p.hx, nv[k][f],
-                        in && vec_ok, xo, yo, 0LL);
+                        in && vec_ok, xany, xo, yo, 0LL);
       if (ragged && in) {
 #pragma unroll
         for (int f = 0; f < NF; ++f)
