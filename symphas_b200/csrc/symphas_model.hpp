@@ -74,6 +74,18 @@ struct ProblemParameters {
   }
 };
 
+// var(N) of PROVISIONAL_DEF (sol/inc/modelmacros.h:682, :1102): a provisional
+// variable is evaluated at every site (and its halo) before the equation and
+// read under derivatives, which is what a staged operand is; declare the
+// provisional expressions as the staged operands of SP_MODEL_STAGED, e.g.
+// SymPhas's MBB (examples/models/modeldefinitions.h:150-155):
+//   SP_MODEL_STAGED(MBB, 1, 1, -bilap(op<1>()) + lap(var<1>()), Lit(),
+//                   -(c<1>() - Lit(4.0) * c<2>() * op<1>() * op<1>()) * op<1>())
+template <int N>
+__host__ __device__ constexpr auto var() {
+  return stage<N - 1>();
+}
+
 namespace detail {
 inline int next_model_id() {
   static std::atomic<int> id{1000};  // ids of user models, above the built-in ones

@@ -1,36 +1,58 @@
-// A user-written model through the C++ front end (symphas_model.hpp): Allen-Cahn
-// (SymPhas's MA, examples/models/modeldefinitions.h:43-46) in the order of
-// SymPhas's printed scheme V^2(psi) - psi^3 + psi, FP64, exact form, run with
-// find_solution; the final field is written to the file named on the command
-// line (raw doubles, x fastest) for the test to compare with the CPU oracle.
+// User-written models through the C++ front end (symphas_model.hpp), FP64, run
+// with find_solution; the final field is written to the file named on the
+// command line (raw doubles, x fastest) for the tests to compare with the CPU
+// oracle.
+//   ma:  Allen-Cahn (SymPhas's MA, examples/models/modeldefinitions.h:43-46) in
+//        the order of SymPhas's printed scheme V^2(psi) - psi^3 + psi, exact form
+//   mbb: SymPhas's MBB (modeldefinitions.h:150-155), model B through a
+//        provisional variable var(1) = -(c1 - 4 c2 psi^2) psi, fused form
 //
-//   user_model <out> <n> <h> <dt> <steps> <seed> <lo> <hi>
+//   user_model <ma|mbb> <out> <n> <h> <dt> <steps> <seed> <lo> <hi>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 
 #include "symphas_model.hpp"
 
 using namespace symphas_b200;
 
 SP_MODEL(MA, 1, lap(op<1>()) + (-(c<2>() * power<3>(op<1>())) + c<1>() * op<1>()));
+SP_MODEL_STAGED(MBB, 1, 1, -bilap(op<1>()) + lap(var<1>()), Lit(),
+                -(c<1>() - Lit(4.0) * c<2>() * op<1>() * op<1>()) * op<1>());
 
-int main(int argc, char** argv) {
-  if (argc != 9) {
-    std::fprintf(stderr, "usage: %s out n h dt steps seed lo hi\n", argv[0]);
-    return 2;
-  }
-  const int n = std::atoi(argv[2]), steps = std::atoi(argv[5]);
-  const double h = std::atof(argv[3]), dt = std::atof(argv[4]);
-  const double lo = std::atof(argv[7]), hi = std::atof(argv[8]);
-  const unsigned long long seed = std::strtoull(argv[6], nullptr, 10);
-  const double coeff[2] = {1.0, 1.0};
-  model_t<MA, SolverFT<Stencil2d2h<5, 6, 13>, true>, 2> m(coeff, 2, ProblemParameters<2>{{n, n}, h});
+template <class M>
+int run(M& m, const char* out, unsigned long long seed, double lo, double hi, double dt,
+        int steps) {
   m.fill_uniform(0, seed, lo, hi);
   find_solution(m, dt, steps);
-  const std::vector<double> psi = m.get_field<0>();
-  FILE* f = std::fopen(argv[1], "wb");
+  const std::vector<double> psi = m.template get_field<0>();
+  FILE* f = std::fopen(out, "wb");
   if (!f || std::fwrite(psi.data(), sizeof(double), psi.size(), f) != psi.size()) return 1;
   std::fclose(f);
   std::printf("index %d time %.6f\n", m.get_index(), m.get_time());
   return 0;
+}
+
+int main(int argc, char** argv) {
+  if (argc != 10) {
+    std::fprintf(stderr, "usage: %s ma|mbb out n h dt steps seed lo hi\n", argv[0]);
+    return 2;
+  }
+  const std::string which = argv[1];
+  const int n = std::atoi(argv[3]), steps = std::atoi(argv[6]);
+  const double h = std::atof(argv[4]), dt = std::atof(argv[5]);
+  const double lo = std::atof(argv[8]), hi = std::atof(argv[9]);
+  const unsigned long long seed = std::strtoull(argv[7], nullptr, 10);
+  const ProblemParameters<2> params{{n, n}, h};
+  if (which == "ma") {
+    const double coeff[2] = {1.0, 1.0};
+    model_t<MA, SolverFT<Stencil2d2h<5, 6, 13>, true>, 2> m(coeff, 2, params);
+    return run(m, argv[2], seed, lo, hi, dt, steps);
+  }
+  if (which == "mbb") {
+    const double coeff[2] = {1.0, 0.25};  // var(1) = psi^3 - psi: model B
+    model_t<MBB, SolverFT<Stencil2d2h<5, 6, 13>, false>, 2> m(coeff, 2, params);
+    return run(m, argv[2], seed, lo, hi, dt, steps);
+  }
+  return 2;
 }

@@ -1,8 +1,9 @@
-"""The C++ front end (symphas_b200/csrc/symphas_model.hpp): a model written by
-the user as an EVOLUTION expression in C++, compiled with the runtime sources
-(tests/cpp/user_model.cu, built by __graft_entry__.build), runs through
-model_t / find_solution and matches the CPU oracle bit for bit in FP64 --
-SymPhas's model A config, 64^2, dx 0.5, dt 0.01, 1000 steps."""
+"""The C++ front end (symphas_b200/csrc/symphas_model.hpp): models written by
+the user as EVOLUTION expressions in C++, compiled with the runtime sources
+(tests/cpp/user_model.cu, built by __graft_entry__.build), run through
+model_t / find_solution: model A matches the CPU oracle bit for bit in FP64
+(SymPhas's model A config, 64^2, dx 0.5, dt 0.01, 1000 steps), and a model
+with a provisional variable matches the oracle's equivalent model."""
 import os
 import subprocess
 
@@ -21,11 +22,27 @@ def test_user_model_matches_the_oracle(tmp_path):
         pytest.fail("tests/cpp/user_model is not built (run __graft_entry__.build())")
     n, h, dt, steps, seed, lo, hi = 64, 0.5, 0.01, 1000, 11, -0.1, 0.1
     out = tmp_path / "psi.bin"
-    r = subprocess.run([EXE, str(out), str(n), str(h), str(dt), str(steps), str(seed), str(lo),
-                        str(hi)], capture_output=True, text=True, timeout=120)
+    r = subprocess.run([EXE, "ma", str(out), str(n), str(h), str(dt), str(steps), str(seed),
+                        str(lo), str(hi)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
     assert "index %d" % steps in r.stdout
     got = np.fromfile(out, dtype=np.float64).reshape(n, n)
     ref = spo.run(spo.make_desc(2, (n, n), spo.MODEL_A, h, dt),
                   spo.seed_uniform(seed, lo, hi, n * n).reshape(n, n), steps)
     assert np.array_equal(got, ref)
+
+
+def test_provisional_variable_model(tmp_path):
+    """SymPhas's MBB (a provisional variable var(1) = -(c1 - 4 c2 psi^2) psi,
+    dpsi = -bilap(psi) + lap(var(1))), with c1 = 1 and c2 = 1/4 model B, run
+    with the provisional variable as a staged operand: within 1e-10 of the
+    oracle's model B (the same scheme in another rounding order)."""
+    n, h, dt, steps, seed, lo, hi = 48, 1.0, 0.005, 300, 21, -0.4, 0.2
+    out = tmp_path / "psi.bin"
+    r = subprocess.run([EXE, "mbb", str(out), str(n), str(h), str(dt), str(steps), str(seed),
+                        str(lo), str(hi)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(out, dtype=np.float64).reshape(n, n)
+    ref = spo.run(spo.make_desc(2, (n, n), spo.MODEL_B, h, dt),
+                  spo.seed_uniform(seed, lo, hi, n * n).reshape(n, n), steps)
+    assert float(np.max(np.abs(got - ref)) / np.max(np.abs(ref))) <= 1e-10
