@@ -220,6 +220,13 @@ int sp_structure_factor(sp_handle* h, int inst, int field, int threshold, double
  * even. */
 int sp_conv3x3_fwd(const void* x, const void* w, const float* bias, const void* res, void* z,
                    void* a, int n, int h, int w_, int cin, int cout, void* stream);
+/* The same convolution on the 5th-generation tensor cores (tcgen05.mma, fp32
+ * accumulator in tensor memory): cin a multiple of 8, cout 32 or a multiple of
+ * 64.  Its waits are bounded; a CTA that gives up sets a device flag, which
+ * sp_conv_tc_status reads (after a device synchronize) and clears. */
+int sp_conv3x3_fwd_tc(const void* x, const void* w, const float* bias, const void* res, void* z,
+                      void* a, int n, int h, int w_, int cin, int cout, void* stream);
+int sp_conv_tc_status(int* gave_up);
 /* dw [cout][3][3][cin] (fp32) += weight gradient of that convolution for the
  * output gradient dy [n][h][w][cout]; cin a multiple of 32, cout of 8. */
 int sp_conv3x3_wgrad(const void* x, const void* dy, float* dw, int n, int h, int w_, int cin,

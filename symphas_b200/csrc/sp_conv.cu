@@ -423,3 +423,287 @@ int sp_adam_step(float* w, void* wb, const float* g, float* m, float* v, long lo
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The forward convolution on the 5th-generation tensor cores (tcgen05): the
+// same implicit GEMM, a 128-pixel x BN-channel tile per CTA with its fp32
+// accumulator in tensor memory.  Operands are gathered by cp.async (the
+// circular wrap in the address) into shared memory in the K-major canonical
+// layout without swizzle -- 8-row x 16-byte core matrices, K-adjacent core
+// matrices 128 B apart (leading byte offset), row-adjacent ones 1 KiB apart
+// (stride byte offset) -- in a ring of stages with a full and an empty
+// mbarrier each; one thread issues the MMAs (M = 128, N = BN, K = 16 each,
+// bf16 x bf16 -> fp32) of a stage once its copies have landed and commits
+// them to the stage's empty barrier, whose (bounded) wait releases the stage
+// to the producers.  Four warps read the accumulator back with tcgen05.ld for
+// the epilogue.  The descriptor fields follow the PTX ISA's shared-memory and
+// instruction descriptors for tcgen05.mma (as CUTLASS's cute/arch headers
+// spell them out).
+// ---------------------------------------------------------------------------
+#include "sp_tma.cuh"
+
+namespace sp {
+namespace conv {
+
+constexpr int TC_BM = 128, TC_BK = 64;
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  // K-major, no swizzle: start >> 4, LBO = 128 B, SBO = 1024 B, version 1
+  return uint64_t((saddr >> 4) & 0x3FFF) | (uint64_t(128 >> 4) << 16) |
+         (uint64_t(1024 >> 4) << 32) | (uint64_t(1) << 46);
+}
+
+template <int BN>
+__device__ __forceinline__ constexpr uint32_t umma_idesc() {
+  // D fp32, A and B bf16, both K-major, N >> 3, M >> 4
+  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(BN >> 3) << 17) |
+         (uint32_t(TC_BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+          tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15])
+      : "r"(addr));
+}
+
+template <int BN>
+struct TcTile {
+  // stages per CTA: about 100 KB of ring, so that two CTAs share an SM (one's
+  // epilogue overlaps the other's main loop)
+  static constexpr int S = BN == 32 ? 5 : BN == 64 ? 4 : 3;
+  static constexpr int A_BYTES = TC_BM * TC_BK * 2, B_BYTES = BN * TC_BK * 2;
+  static constexpr int STAGE = A_BYTES + B_BYTES;
+  static constexpr int NBAR = 2 * S + 1;  // full[S], empty[S], done
+  static constexpr int SMEM = S * STAGE + NBAR * 8 + 16;
+  static constexpr int COLS = BN;  // TMEM columns (a power of two >= 32)
+};
+
+// Warp roles (160 threads): warps 0-3 gather the operands of each K step
+// (64 taps x channels) into the stage ring, arriving on full[s] as their
+// copies land (cp.async.mbarrier.arrive.noinc), and after the main loop read
+// the accumulator back (warp w: TMEM lanes 32w..32w+31 = pixels) for the
+// epilogue; warp 4 allocates the tensor memory and one of its threads issues
+// the MMAs of each stage once full[s] completes, committing to empty[s] (the
+// stage may be refilled) and, after the last, to done.
+template <int BN>
+__global__ void __launch_bounds__(160) k_conv3x3_fwd_tc(const FwdParams p, int* err) {
+  using TT = TcTile<BN>;
+  constexpr int S = TT::S;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * TT::STAGE);
+  uint64_t* empty = full + S;
+  uint64_t* done = empty + S;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long npix = (long long)p.n * p.h * p.wid;
+  const long long p0 = (long long)blockIdx.x * TC_BM;
+  const int co0 = blockIdx.y * BN;
+  const int K = 9 * p.cin, nk = (K + TC_BK - 1) / TC_BK;
+
+  if (warp == 4) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(TT::COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      tma::mbar_init(&full[s], 128);
+      tma::mbar_init(&empty[s], 1);
+    }
+    tma::mbar_init(done, 1);
+    tma::fence_barrier_init();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  bool bad = false;
+
+  if (warp < 4) {
+    // producer: this thread's k chunk (8 channels) j of every K step, its 8
+    // pixel rows tid / 8 + 16 i of A and BN / 16 channel rows of B
+    const int j = tid & 7;
+    int ry[8], rx[8];
+    long long rbase[8];
+    bool rok[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const long long pix = p0 + (tid >> 3) + 16 * i;
+      rok[i] = pix < npix;
+      const long long pp = rok[i] ? pix : 0;
+      rx[i] = int(pp % p.wid);
+      ry[i] = int((pp / p.wid) % p.h);
+      rbase[i] = (pp / ((long long)p.wid * p.h)) * p.h * p.wid;
+    }
+    for (int ks = 0; ks < nk; ++ks) {
+      const int s = ks % S;
+      if (ks >= S) bad |= !tma::mbar_wait(&empty[s], uint32_t((ks / S - 1) & 1));
+      unsigned char* sa = smem + s * TT::STAGE;
+      unsigned char* sb = sa + TT::A_BYTES;
+      const int k = ks * TC_BK + j * 8;
+      const bool kok = k < K;
+      const int tap = kok ? k / p.cin : 0, c = kok ? k - tap * p.cin : 0;
+      const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int r = (tid >> 3) + 16 * i;
+        int yy = ry[i] + dy, xx = rx[i] + dx;
+        yy += (yy < 0) ? p.h : 0;
+        yy -= (yy >= p.h) ? p.h : 0;
+        xx += (xx < 0) ? p.wid : 0;
+        xx -= (xx >= p.wid) ? p.wid : 0;
+        const __nv_bfloat16* src = p.x + ((rbase[i] + (long long)yy * p.wid + xx) * p.cin + c);
+        cp_async16(sa + (r >> 3) * 1024 + j * 128 + (r & 7) * 16, src, rok[i] && kok);
+      }
+#pragma unroll
+      for (int i = 0; i < BN / 16; ++i) {
+        const int r = (tid >> 3) + 16 * i;
+        const __nv_bfloat16* src = p.w + ((long long)(co0 + r) * K + (kok ? k : 0));
+        cp_async16(sb + (r >> 3) * 1024 + j * 128 + (r & 7) * 16, src, kok);
+      }
+      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(
+                       smem_u32(&full[s]))
+                   : "memory");
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+
+    // epilogue: accumulator rows (pixels) 32 warp .. 32 warp + 31
+    bad |= !tma::mbar_wait(done, 0);
+    __syncwarp();  // tcgen05.ld is warp-collective
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const long long pix = p0 + 32 * warp + lane;
+#pragma unroll
+    for (int c16 = 0; c16 < BN / 16; ++c16) {
+      uint32_t v[16];
+      tmem_ld16(tmem + (uint32_t(32 * warp) << 16) + uint32_t(c16 * 16), v);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (pix < npix && !bad) {
+        const int cob = co0 + c16 * 16;
+        const long long o = pix * p.cout + cob;
+        __align__(16) __nv_bfloat162 zz[8], aa[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          float v0 = __uint_as_float(v[2 * e]), v1 = __uint_as_float(v[2 * e + 1]);
+          if (p.bias) {
+            v0 += p.bias[cob + 2 * e];
+            v1 += p.bias[cob + 2 * e + 1];
+          }
+          if (p.res) {
+            const __nv_bfloat162 r = *reinterpret_cast<const __nv_bfloat162*>(p.res + o + 2 * e);
+            v0 += __bfloat162float(r.x);
+            v1 += __bfloat162float(r.y);
+          }
+          zz[e] = __floats2bfloat162_rn(v0, v1);
+          if (p.a) aa[e] = __floats2bfloat162_rn(gelu(v0), gelu(v1));
+        }
+        if (p.z) {
+          reinterpret_cast<uint4*>(p.z + o)[0] = reinterpret_cast<const uint4*>(zz)[0];
+          reinterpret_cast<uint4*>(p.z + o)[1] = reinterpret_cast<const uint4*>(zz)[1];
+        }
+        if (p.a) {
+          reinterpret_cast<uint4*>(p.a + o)[0] = reinterpret_cast<const uint4*>(aa)[0];
+          reinterpret_cast<uint4*>(p.a + o)[1] = reinterpret_cast<const uint4*>(aa)[1];
+        }
+      }
+    }
+  } else if (lane == 0) {
+    // MMA issuer
+    constexpr uint32_t idesc = umma_idesc<BN>();
+    for (int ks = 0; ks < nk; ++ks) {
+      const int s = ks % S;
+      bad |= !tma::mbar_wait(&full[s], uint32_t((ks / S) & 1));
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(smem + s * TT::STAGE);
+      const uint32_t b0 = a0 + TT::A_BYTES;
+#pragma unroll
+      for (int kk = 0; kk < TC_BK / 16; ++kk)
+        umma_bf16(tmem, umma_desc(a0 + kk * 256), umma_desc(b0 + kk * 256), idesc,
+                  (ks > 0 || kk > 0) ? 1u : 0u);
+      umma_commit(&empty[s]);
+    }
+    umma_commit(done);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 4)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TT::COLS));
+  if (bad) atomicExch(err, 1);
+}
+
+// device flag set by a tcgen05 CTA that gave up on a wait (allocated once)
+int* tc_error_flag() {
+  static int* e = [] {
+    int* f = nullptr;
+    if (cudaMalloc(&f, sizeof(int)) != cudaSuccess) return static_cast<int*>(nullptr);
+    cudaMemset(f, 0, sizeof(int));
+    return f;
+  }();
+  return e;
+}
+
+}  // namespace conv
+}  // namespace sp
+
+extern "C" int sp_conv_tc_status(int* gave_up) {
+  int* err = sp::conv::tc_error_flag();
+  if (!err || !gave_up) return SP_EINVAL;
+  if (cudaDeviceSynchronize() != cudaSuccess) return SP_ECUDA;
+  if (cudaMemcpy(gave_up, err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return SP_ECUDA;
+  return cudaMemset(err, 0, sizeof(int)) == cudaSuccess ? SP_OK : SP_ECUDA;
+}
+
+namespace sp {
+namespace conv {
+template <int BN>
+int launch_fwd_tc(const FwdParams& p, int* err, cudaStream_t s) {
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      k_conv3x3_fwd_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcTile<BN>::SMEM);
+  if (attr != cudaSuccess) return SP_ECUDA;
+  const long long npix = (long long)p.n * p.h * p.wid;
+  k_conv3x3_fwd_tc<BN><<<dim3(unsigned((npix + TC_BM - 1) / TC_BM), unsigned(p.cout / BN)), 160,
+                         TcTile<BN>::SMEM, s>>>(p, err);
+  return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ECUDA;
+}
+}  // namespace conv
+}  // namespace sp
+
+extern "C" int sp_conv3x3_fwd_tc(const void* x, const void* w, const float* bias, const void* res,
+                                 void* z, void* a, int n, int h, int w_, int cin, int cout,
+                                 void* stream) {
+  using namespace sp::conv;
+  if (!x || !w || (!z && !a) || n < 1 || h < 1 || w_ < 1 || cin % 8 != 0 || cin < 8 ||
+      !(cout == 32 || cout % 64 == 0))
+    return SP_EINVAL;
+  int* err = tc_error_flag();
+  if (!err) return SP_ENOMEM;
+  FwdParams p{static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w), bias,
+              static_cast<const __nv_bfloat16*>(res), static_cast<__nv_bfloat16*>(z),
+              static_cast<__nv_bfloat16*>(a), n, h, w_, cin, cout};
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cout == 32) return launch_fwd_tc<32>(p, err, s);
+  if (cout % 128 == 0) return launch_fwd_tc<128>(p, err, s);
+  return launch_fwd_tc<64>(p, err, s);
+}

@@ -7,9 +7,11 @@ channels at 256^2 / 128^2 / 64^2 / 32^2, 3x3 kernels, GELU, additive skips,
 prediction is projected onto zero mean, so every jump conserves the mass of
 psi exactly as model B does.  Convolutions, their gradients and the Adam
 update run in this package's BF16 tensor-core kernels
-(sp_conv3x3_fwd / sp_conv3x3_wgrad / sp_conv3x3_flip / sp_adam_step, fp32
-accumulation, fp32 master weights); PyTorch holds the tensors and does the
-element-wise glue (GELU, pooling, up-sampling, the loss).
+(sp_conv3x3_fwd_tc on tcgen05 with the accumulator in tensor memory, or
+sp_conv3x3_fwd on mma.sync; sp_conv3x3_wgrad / sp_conv3x3_flip /
+sp_adam_step; fp32 accumulation, fp32 master weights); PyTorch holds the
+tensors and does the element-wise glue (pooling, up-sampling, the loss, and
+GELU under autograd -- at inference the convolution's epilogue applies it).
 
 Training data are trajectories of this package's own fused FD kernel
 (model_MB_t, batch of instances in one persistent launch).  At inference each
@@ -44,6 +46,24 @@ def _s():
 def _ok(rc, what):
     if rc != C.SP_OK:
         raise C.SymPhasError(rc, what)
+
+
+# True: forward convolutions on the tcgen05 kernel (tensor-memory accumulator)
+# where its shapes allow (cin % 8 == 0, cout 32 or a multiple of 64).  Off by
+# default: its im2col gather re-reads each input pixel once per tap, and on the
+# network's shapes it runs at 54-171 TFLOP/s against the mma.sync kernel's
+# 72-190, so mma.sync stays the default.
+USE_TC = False
+
+
+def _fwd(x, wb, bias, res, z, a, ci, co):
+    n, h, w = x.shape[:3]
+    if USE_TC and ci % 8 == 0 and (co == 32 or co % 64 == 0):
+        _ok(C.lib().sp_conv3x3_fwd_tc(_p(x), _p(wb), _p(bias), _p(res), _p(z), _p(a), n, h, w,
+                                      ci, co, _s()), "sp_conv3x3_fwd_tc")
+    else:
+        _ok(C.lib().sp_conv3x3_fwd(_p(x), _p(wb), _p(bias), _p(res), _p(z), _p(a), n, h, w, ci,
+                                   co, _s()), "sp_conv3x3_fwd")
 
 
 class ConvLayer:
@@ -89,8 +109,7 @@ class _Conv(torch.autograd.Function):
     def forward(ctx, x, anchor, layer, res):
         n, h, w, ci = x.shape
         z = torch.empty(n, h, w, layer.cout, device="cuda", dtype=torch.bfloat16)
-        _ok(C.lib().sp_conv3x3_fwd(_p(x), _p(layer.wb), _p(layer.b), _p(res), _p(z), None, n, h,
-                                   w, ci, layer.cout, _s()), "sp_conv3x3_fwd")
+        _fwd(x, layer.wb, layer.b, res, z, None, ci, layer.cout)
         ctx.save_for_backward(x)
         ctx.layer = layer
         ctx.has_res = res is not None
@@ -109,8 +128,7 @@ class _Conv(torch.autograd.Function):
         if ctx.needs_input_grad[0]:
             _ok(C.lib().sp_conv3x3_flip(_p(L.wb), _p(L.wf), ci, L.cout, _s()), "sp_conv3x3_flip")
             dx = torch.empty_like(x)
-            _ok(C.lib().sp_conv3x3_fwd(_p(dz), _p(L.wf), None, None, _p(dx), None, n, h, w,
-                                       L.cout, ci, _s()), "sp_conv3x3_fwd")
+            _fwd(dz, L.wf, None, None, dx, None, L.cout, ci)
         return dx, None, None, (dz if ctx.has_res else None)
 
 
@@ -120,6 +138,17 @@ def conv(x, layer, res=None):
 
 def gelu(z):
     return F.gelu(z, approximate="tanh")
+
+
+def conv_gelu(x, layer, res=None):
+    """gelu(conv(x) + bias (+ res)); without autograd, one kernel writes the
+    activation from its epilogue."""
+    if torch.is_grad_enabled():
+        return gelu(conv(x, layer, res))
+    n, h, w, ci = x.shape
+    a = torch.empty(n, h, w, layer.cout, device="cuda", dtype=torch.bfloat16)
+    _fwd(x, layer.wb, layer.b, res, None, a, ci, layer.cout)
+    return a
 
 
 def pool2(x):
@@ -168,13 +197,13 @@ class JumpNet:
         x[..., 0] = psi.bfloat16()
         skips = []
         for lvl, (a, b) in enumerate(self.enc):
-            x = gelu(conv(gelu(conv(x, a)), b))
+            x = conv_gelu(conv_gelu(x, a), b)
             if lvl < len(self.enc) - 1:
                 skips.append(x)
                 x = pool2(x)
         for (a, b), s in zip(self.dec, reversed(skips)):
-            x = gelu(conv(up2(x), a, res=s))
-            x = gelu(conv(x, b))
+            x = conv_gelu(up2(x), a, res=s)
+            x = conv_gelu(x, b)
         d = conv(x, self.head)[..., 0].float()
         d = d - d.mean((1, 2), keepdim=True)  # exact mass conservation
         return d * self.scale

@@ -1,0 +1,114 @@
+"""The tcgen05 forward convolution (fp32 accumulator in tensor memory) against
+the plain PyTorch fp32 reference on the same bf16 operands, and against the
+mma.sync kernel it can replace: the epilogue (bias, residual, GELU), ragged
+pixel counts (not a multiple of the 128-pixel tile), a partial last K step
+(cin = 8: K = 72), both output widths (cout 32 and multiples of 64), and the
+bounded waits' flag left clear.
+
+Tolerances: both kernels accumulate in fp32, so their sums agree to ~1e-6
+relative before the bf16 rounding of the stored outputs; outputs are compared
+with the reference at 1.5e-2 relative to their scale and with each other at
+2^-7 relative (one bf16 rounding step either way)."""
+import ctypes
+
+import pytest
+import torch
+import torch.nn.functional as F
+
+from symphas_b200 import _capi as C
+
+pytestmark = pytest.mark.gpu
+
+
+def ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def ref_conv(x, w, b=None):
+    xp = F.pad(x.permute(0, 3, 1, 2), (1, 1, 1, 1), mode="circular")
+    return F.conv2d(xp, w.permute(0, 3, 1, 2), b).permute(0, 2, 3, 1)
+
+
+def rel(a, b):
+    return float((a - b).abs().max() / b.abs().max().clamp_min(1e-30))
+
+
+def status():
+    flag = ctypes.c_int(-1)
+    assert C.lib().sp_conv_tc_status(ctypes.byref(flag)) == C.SP_OK
+    return flag.value
+
+
+@pytest.mark.parametrize("n,h,w,ci,co", [(2, 16, 24, 32, 64), (1, 9, 7, 64, 32),
+                                         (1, 8, 8, 128, 256), (3, 33, 17, 32, 32),
+                                         (1, 10, 10, 8, 64), (2, 64, 64, 64, 128)])
+def test_tc_forward_matches_reference_and_mma_sync(n, h, w, ci, co):
+    torch.manual_seed(0)
+    x = torch.randn(n, h, w, ci, device="cuda").bfloat16()
+    wt = (torch.randn(co, 3, 3, ci, device="cuda") / (3 * ci ** 0.5)).bfloat16()
+    b = torch.randn(co, device="cuda") * 0.1
+    res = torch.randn(n, h, w, co, device="cuda").bfloat16()
+    z = torch.full((n, h, w, co), float("nan"), device="cuda", dtype=torch.bfloat16)
+    a = torch.full_like(z, float("nan"))
+    rc = C.lib().sp_conv3x3_fwd_tc(ptr(x), ptr(wt), ptr(b), ptr(res), ptr(z), ptr(a), n, h, w,
+                                   ci, co, stream())
+    assert rc == C.SP_OK
+    assert status() == 0
+    zr = ref_conv(x.float(), wt.float(), b) + res.float()
+    assert not torch.isnan(z).any() and not torch.isnan(a).any()
+    assert rel(z.float(), zr) < 1.5e-2
+    assert rel(a.float(), F.gelu(zr, approximate="tanh")) < 1.5e-2
+    if ci % 32 == 0:
+        z2 = torch.empty_like(z)
+        assert C.lib().sp_conv3x3_fwd(ptr(x), ptr(wt), ptr(b), ptr(res), ptr(z2), None, n, h, w,
+                                      ci, co, stream()) == C.SP_OK
+        torch.cuda.synchronize()
+        assert rel(z.float(), z2.float()) < 2.0 ** -7
+
+
+def test_tc_forward_single_output_and_no_epilogue_operands():
+    torch.manual_seed(2)
+    n, h, w, ci, co = 1, 12, 20, 32, 64
+    x = torch.randn(n, h, w, ci, device="cuda").bfloat16()
+    wt = (torch.randn(co, 3, 3, ci, device="cuda") / (3 * ci ** 0.5)).bfloat16()
+    a = torch.empty(n, h, w, co, device="cuda", dtype=torch.bfloat16)
+    assert C.lib().sp_conv3x3_fwd_tc(ptr(x), ptr(wt), None, None, None, ptr(a), n, h, w, ci, co,
+                                     stream()) == C.SP_OK
+    assert status() == 0
+    zr = ref_conv(x.float(), wt.float())
+    assert rel(a.float(), F.gelu(zr, approximate="tanh")) < 1.5e-2
+
+
+def test_tc_forward_rejects_unsupported_shapes():
+    x = torch.zeros(1, 4, 4, 32, device="cuda", dtype=torch.bfloat16)
+    wt = torch.zeros(48, 3, 3, 32, device="cuda", dtype=torch.bfloat16)
+    z = torch.zeros(1, 4, 4, 48, device="cuda", dtype=torch.bfloat16)
+    assert C.lib().sp_conv3x3_fwd_tc(ptr(x), ptr(wt), None, None, ptr(z), None, 1, 4, 4, 32, 48,
+                                     stream()) == C.SP_EINVAL
+    assert C.lib().sp_conv3x3_fwd_tc(ptr(x), ptr(wt), None, None, ptr(z), None, 1, 4, 4, 12, 64,
+                                     stream()) == C.SP_EINVAL
+
+
+def test_surrogate_network_on_either_kernel():
+    """The jump network gives the same prediction with its forward
+    convolutions on tcgen05 or on mma.sync (bf16 activations: 2e-2)."""
+    from symphas_b200 import surrogate as S
+
+    torch.cuda.set_device(0)
+    net = S.JumpNet((32, 64, 128))
+    psi = torch.rand(2, 64, 64, device="cuda") - 0.5
+    old = S.USE_TC
+    try:
+        with torch.no_grad():
+            S.USE_TC = False
+            d0 = net(psi)
+            S.USE_TC = True
+            d1 = net(psi)
+    finally:
+        S.USE_TC = old
+    assert status() == 0
+    assert rel(d1, d0) < 2e-2
