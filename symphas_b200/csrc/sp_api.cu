@@ -46,16 +46,18 @@ const std::vector<KernelInfo>* find_kernels(const KernelKey& key) {
   auto it = table().find(tup(key));
   return it == table().end() ? nullptr : &it->second;
 }
-// the built-in kernel sets (sp_inst_exact.cu, sp_inst_fused.cu); weak, so a
-// program that compiles this runtime with only its own models (the C++ front
-// end, symphas_model.hpp) links without them
+// the built-in kernel sets (sp_inst_exact.cu, sp_inst_fused.cu,
+// sp_inst_wide.cu); weak, so a program that compiles this runtime with only
+// its own models (the C++ front end, symphas_model.hpp) links without them
 void register_exact_kernels() __attribute__((weak));
 void register_fused_kernels() __attribute__((weak));
+void register_wide_kernels() __attribute__((weak));
 void register_all_kernels() {
   static std::once_flag once;
   std::call_once(once, [] {
     if (register_exact_kernels) register_exact_kernels();
     if (register_fused_kernels) register_fused_kernels();
+    if (register_wide_kernels) register_wide_kernels();
   });
 }
 

@@ -77,6 +77,31 @@ __device__ __forceinline__ Vec<float, 2> fma_op(const Vec<float, 2>& a, const Ve
                                                  const Vec<float, 2>& c) {
   return v2(__ffma2_rn(f2(a), f2(b), f2(c)));
 }
+// four FP32 lanes: two packed instructions, lanes (0, 1) and (2, 3)
+__device__ __forceinline__ float2 lo2(const Vec<float, 4>& a) { return make_float2(a.v[0], a.v[1]); }
+__device__ __forceinline__ float2 hi2(const Vec<float, 4>& a) { return make_float2(a.v[2], a.v[3]); }
+__device__ __forceinline__ Vec<float, 4> v4(float2 l, float2 h) {
+  Vec<float, 4> r;
+  r.v[0] = l.x;
+  r.v[1] = l.y;
+  r.v[2] = h.x;
+  r.v[3] = h.y;
+  return r;
+}
+__device__ __forceinline__ Vec<float, 4> operator+(const Vec<float, 4>& a, const Vec<float, 4>& b) {
+  return v4(__fadd2_rn(lo2(a), lo2(b)), __fadd2_rn(hi2(a), hi2(b)));
+}
+__device__ __forceinline__ Vec<float, 4> operator-(const Vec<float, 4>& a, const Vec<float, 4>& b) {
+  return v4(__fadd2_rn(lo2(a), make_float2(-b.v[0], -b.v[1])),
+            __fadd2_rn(hi2(a), make_float2(-b.v[2], -b.v[3])));
+}
+__device__ __forceinline__ Vec<float, 4> operator*(const Vec<float, 4>& a, const Vec<float, 4>& b) {
+  return v4(__fmul2_rn(lo2(a), lo2(b)), __fmul2_rn(hi2(a), hi2(b)));
+}
+__device__ __forceinline__ Vec<float, 4> fma_op(const Vec<float, 4>& a, const Vec<float, 4>& b,
+                                                 const Vec<float, 4>& c) {
+  return v4(__ffma2_rn(lo2(a), lo2(b), lo2(c)), __ffma2_rn(hi2(a), hi2(b), hi2(c)));
+}
 __device__ __forceinline__ float fma_op(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_op(double a, double b, double c) { return __fma_rn(a, b, c); }
 template <class T, int W>

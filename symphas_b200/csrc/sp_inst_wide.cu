@@ -1,0 +1,31 @@
+/*
+ * sp_inst_wide.cu -- FP32 fused-form kernels with four x-sites per thread
+ * (16-byte shared-memory words, two packed FP32x2 instructions per
+ * operation).  They evaluate every site exactly as the two-site kernels do
+ * and share their field layout, so they are further tile shapes for
+ * sp_autotune (registered after the fused set, in their own translation unit
+ * so that the build compiles them in parallel).
+ */
+#include "sp_launch.cuh"
+
+#define SP_WIDE3(MODEL, MF)                                                         \
+  SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3w1);   \
+  SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3w2);   \
+  SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3w3);   \
+  SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3w4);   \
+  SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3w5);
+#define SP_WIDE2(MODEL, MF0, MF1)                                                   \
+  SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2w1); \
+  SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2w2); \
+  SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2w3);
+
+namespace sp {
+void register_wide_kernels() {
+  SP_WIDE3(SPK_A, MF_A_fused)
+  SP_WIDE3(SPK_B, MF_B_fused)
+  SP_WIDE3(SPK_C, MF_C_fused)
+  SP_WIDE2(SPK_A, MF_A_fused, MF_A_fused)
+  SP_WIDE2(SPK_B, MF_B_fused, MF_B_fused)
+  SP_WIDE2(SPK_ENS_AB, MF_AMK_fused, MF_BMK_fused)
+}
+}  // namespace sp

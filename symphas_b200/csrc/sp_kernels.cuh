@@ -97,11 +97,16 @@ struct TileCfg {
 
 // halo geometry shared by the kernels and the host: x halo HXA covers the
 // stencil reach R and the stage ring (RSA = RS rounded up to W, plus the
-// stage's own reach RI), rounded up to 16 bytes
+// stage's own reach RI), rounded up to 16 bytes.  With W > 2 the ring's column
+// groups are wider than the RS columns the output reads from them: only those
+// RS columns need their stencil inside the halo (RS + RI), the group's other
+// lanes are computed from whatever lies next to the row in shared memory and
+// are never read, so W = 2 and W = 4 tiles share one field layout.
 template <class T, int W, int R, int NS, int RS, int RI>
 struct HaloGeom {
   static constexpr int RSA = NS > 0 ? ceil_to(imax(RS, 1), W) : 0;
-  static constexpr int HXA = ceil_to(imax(imax(R, 1), NS > 0 ? RSA + RI : 0),
+  static constexpr int RX = W > 2 ? imax(RS, 1) : RSA;
+  static constexpr int HXA = ceil_to(imax(imax(R, 1), NS > 0 ? RX + RI : 0),
                                      imax(16 / (int)sizeof(T), W));
 };
 
@@ -187,6 +192,13 @@ __device__ __forceinline__ void st_if(float* p, const Vec<float, 2>& v, bool on)
       "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %3, 0;\n\t"
       "@q st.global.v2.f32 [%0], {%1, %2};\n\t}" ::"l"(p),
       "f"(v.v[0]), "f"(v.v[1]), "r"(int(on))
+      : "memory");
+}
+__device__ __forceinline__ void st_if(float* p, const Vec<float, 4>& v, bool on) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %5, 0;\n\t"
+      "@q st.global.v4.f32 [%0], {%1, %2, %3, %4};\n\t}" ::"l"(p),
+      "f"(v.v[0]), "f"(v.v[1]), "f"(v.v[2]), "f"(v.v[3]), "r"(int(on))
       : "memory");
 }
 __device__ __forceinline__ void st_if(double* p, const Vec<double, 2>& v, bool on) {

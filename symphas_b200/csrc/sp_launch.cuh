@@ -150,6 +150,15 @@ template <> struct Tiles<float> {
   using C3b = TileCfg<64, 16, 2, 2, 2>;
   using C3c = TileCfg<64, 32, 4, 2, 2>;
   using C3d = TileCfg<128, 16, 4, 2, 2>;
+  // four x-sites per thread (16-byte shared-memory words)
+  using D3w1 = TileCfg<128, 8, 2, 2, 4>;
+  using D3w2 = TileCfg<128, 16, 4, 2, 4>;
+  using D3w3 = TileCfg<64, 16, 2, 2, 4>;
+  using D3w4 = TileCfg<128, 16, 2, 2, 4>;
+  using D3w5 = TileCfg<64, 32, 4, 2, 4>;
+  using D2w1 = TileCfg<128, 16, 4, 3, 4>;
+  using D2w2 = TileCfg<128, 32, 4, 2, 4>;
+  using D2w3 = TileCfg<128, 16, 2, 3, 4>;
   using D2b = TileCfg<64, 32, 4, 3, 2>;
   using D2c = TileCfg<128, 32, 8, 2, 2>;
 };

@@ -222,8 +222,10 @@ def test_f32_mass_drift_with_fp64_reduction():
     assert abs(m1 - m0) <= 1e-4 * abs(m0)
 
 
-@pytest.mark.parametrize("dim,n,cls", [(3, 40, sp.model_MB_t), (3, 24, sp.model_MC_t),
-                                       (2, 200, sp.model_MB_t), (2, 136, sp.model_MA_t)])
+@pytest.mark.parametrize("dim,n,cls", [(3, 40, sp.model_MB_t), (3, 42, sp.model_MB_t),
+                                       (3, 24, sp.model_MC_t),
+                                       (2, 200, sp.model_MB_t), (2, 202, sp.model_MB_t),
+                                       (2, 136, sp.model_MA_t)])
 def test_every_tile_shape_gives_the_same_fields(dim, n, cls, monkeypatch):
     """The autotuner may pick any tile shape: each must give the same bits."""
     st = S2 if dim == 2 else S3
