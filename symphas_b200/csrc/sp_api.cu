@@ -354,6 +354,17 @@ int setup_2d_t(sp_handle* H) {
   return SP_OK;
 }
 
+// whether tile variant v can run this handle's grid (row kernels need every
+// instance to be a 3D grid of their x extent, periodic in x)
+bool applicable(const sp_handle* H, int v) {
+  const sp::KernelInfo& k = H->variants[v];
+  if (k.nx_only == 0) return true;
+  if (H->dim != 3 || H->d.boundary[0] != SP_PERIODIC) return false;
+  for (const InstGeo& g : H->geo)
+    if (g.n[0] != k.nx_only) return false;
+  return true;
+}
+
 // TMA descriptors of every field of both buffers (box = the tile plus its
 // halo), output origins, grid sizing and scratch: everything that depends on
 // the chosen tile shape.
@@ -382,7 +393,8 @@ int configure(sp_handle* H, int variant) {
         const InstGeo& g = H->geo[i];
         void* base = field_base(H, k, i, f);
         outs[idx] = base;
-        const cuuint32_t bw = cuuint32_t(H->ki->tx + 2 * H->h[0]);
+        const cuuint32_t bw =
+            cuuint32_t(H->ki->tx + 2 * (H->ki->box_hx < 0 ? H->h[0] : H->ki->box_hx));
         const cuuint32_t bh = cuuint32_t(H->ki->ty + 2 * R);
         const CUtensorMapDataType dt =
             H->esz == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
@@ -576,7 +588,7 @@ int create(const sp_desc* desc, const sp_member* members, int count, sp_handle* 
     if (it != g_tuned.end()) variant = it->second;
   }
   if (const char* t = getenv("SP_TILE")) variant = atoi(t);
-  if (variant < 0 || variant >= int(H->variants.size())) variant = 0;
+  if (variant < 0 || variant >= int(H->variants.size()) || !applicable(H, variant)) variant = 0;
   if (int rc = configure(H, variant)) return rc;
   SP_CUDA(H, cudaDeviceSynchronize());
   return SP_OK;
@@ -908,6 +920,7 @@ int sp_autotune(sp_handle* H, int reps) {
   float best_ms = 1e30f;
   int rc = SP_OK;
   for (int v = 0; v < int(H->variants.size()) && rc == SP_OK; ++v) {
+    if (!applicable(H, v)) continue;
     if ((rc = configure(H, v))) break;
     // right-hand-side launches: the same loads and stores as a step, and the
     // state of the model is left untouched

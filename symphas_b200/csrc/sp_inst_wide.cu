@@ -4,7 +4,8 @@
  * operation).  They evaluate every site exactly as the two-site kernels do
  * and share their field layout, so they are further tile shapes for
  * sp_autotune (registered after the fused set, in their own translation unit
- * so that the build compiles them in parallel).
+ * so that the build compiles them in parallel), together with the row kernels
+ * of the conserved pattern (sp_chrow.cuh).
  */
 #include "sp_launch.cuh"
 
@@ -24,6 +25,15 @@ void register_wide_kernels() {
   SP_WIDE3(SPK_A, MF_A_fused)
   SP_WIDE3(SPK_B, MF_B_fused)
   SP_WIDE3(SPK_C, MF_C_fused)
+  // row kernels of the conserved pattern (x extent 256 or 128, periodic in x)
+  SP_REGCHROW(SPK_B, MF_B_fused, 256, 10, 1, 2, true);
+  SP_REGCHROW(SPK_B, MF_B_fused, 256, 10, 1, 2, false);
+  SP_REGCHROW(SPK_B, MF_B_fused, 256, 18, 1, 2, true);
+  SP_REGCHROW(SPK_B, MF_B_fused, 256, 6, 1, 2, false);
+  SP_REGCHROW(SPK_B, MF_B_fused, 128, 9, 2, 2, true);
+  SP_REGCHROW(SPK_B, MF_B_fused, 128, 18, 1, 2, true);
+  SP_REGCHROW(SPK_BMK, MF_BMK_fused, 256, 10, 1, 2, true);
+  SP_REGCHROW(SPK_BMK, MF_BMK_fused, 128, 9, 2, 2, true);
   SP_WIDE2(SPK_A, MF_A_fused, MF_A_fused)
   SP_WIDE2(SPK_B, MF_B_fused, MF_B_fused)
   SP_WIDE2(SPK_ENS_AB, MF_AMK_fused, MF_BMK_fused)

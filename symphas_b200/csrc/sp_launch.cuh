@@ -4,6 +4,7 @@
 #pragma once
 
 #include "sp_ch.cuh"
+#include "sp_chrow.cuh"
 #include "sp_kernels.cuh"
 #include "sp_models.cuh"
 #include "sp_registry.h"
@@ -65,6 +66,38 @@ struct EntryCh3 {
   static KernelInfo info() {
     return KernelInfo{1, 1, K::R, K::HXA, K::TX, K::TY, K::SPT, K::PD, K::NT, K::SMEM,
                       &launch, &occupancy};
+  }
+};
+
+// the row kernel of the conserved pattern (sp_chrow.cuh): grids of x extent
+// NXR, periodic in x
+template <class MF, int NXR, int YW, int SPT, int PD, bool QP>
+struct EntryChRow {
+  using M = model_of<MF>;
+  using K = ChRow<M, NXR, YW, SPT, PD, QP>;
+  static cudaError_t launch(const void* prm, dim3 grid, cudaStream_t s) {
+    auto kern = k_chrow<M, K>;
+    static cudaError_t attr = cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
+    if (attr != cudaSuccess) return attr;
+    const M m = MF{}();
+    kern<<<grid, K::NT, K::SMEM, s>>>(*static_cast<const StepParams<float>*>(prm), m);
+    return cudaGetLastError();
+  }
+  static int occupancy() {
+    auto kern = k_chrow<M, K>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, K::NT, K::SMEM) != cudaSuccess)
+      return 1;
+    return n > 0 ? n : 1;
+  }
+  static KernelInfo info() {
+    KernelInfo i{1, 1, K::R, K::HXA, K::TX, K::TY, K::SPT, K::PD, K::NT, K::SMEM,
+                 &launch, &occupancy};
+    i.box_hx = 0;
+    i.nx_only = NXR;
+    return i;
   }
 };
 
@@ -177,6 +210,9 @@ template <> struct Tiles<double> {
 #define SP_REG3T(MODEL, FORM, MF, T, DT, LP, GP, BP, TILE)                  \
   ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 3, DT, LP, GP, BP},    \
                         ::sp::Entry3<::sp::MF, T, LP, GP, BP, TILE, FORM == SPK_EXACT>::info())
+#define SP_REGCHROW(MODEL, MF, NXR, YW, SPT, PD, QP)                            \
+  ::sp::register_kernel(::sp::KernelKey{MODEL, SPK_FUSED, 3, 0, 7, 10, 25},      \
+                        ::sp::EntryChRow<::sp::MF, NXR, YW, SPT, PD, QP>::info())
 #define SP_REGCH3(MODEL, MF, TILE)                                          \
   ::sp::register_kernel(::sp::KernelKey{MODEL, SPK_FUSED, 3, 0, 7, 10, 25},  \
                         ::sp::EntryCh3<::sp::MF, float, TILE>::info())

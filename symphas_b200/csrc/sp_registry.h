@@ -35,6 +35,11 @@ struct KernelInfo {
   cudaError_t (*launch)(const void* params, dim3 grid, cudaStream_t s);
   // CTAs of this kernel resident per SM (for sizing grids)
   int (*occupancy)();
+  // x halo inside the TMA box (-1: the field's x halo); a kernel that takes
+  // its x neighbours from elsewhere loads the bare rows
+  int box_hx = -1;
+  // nonzero: the kernel runs only on 3D grids of this x extent, periodic in x
+  int nx_only = 0;
 };
 
 // appends a tile variant for `key` (the first registered is the default)

@@ -239,7 +239,10 @@ def test_every_tile_shape_gives_the_same_fields(dim, n, cls, monkeypatch):
         monkeypatch.setenv("SP_TILE", str(v))
         m = cls(dim, sp.SolverFT(st, form="fused"), sp.ProblemParameters(dims, h=1.0),
                 coeff=coeff, dtype="f32")
-        assert m.kernel_info()["variant"] == v
+        if m.kernel_info()["variant"] != v:  # a row kernel of another x extent
+            assert v > 0 and m.kernel_info()["variant"] == 0
+            m.close()
+            continue
         for f in range(cls.nfields):
             m.fill_uniform(f, 60 + f, -0.3, 0.1)
         m.step(0.004, 25)
@@ -252,3 +255,42 @@ def test_every_tile_shape_gives_the_same_fields(dim, n, cls, monkeypatch):
     monkeypatch.delenv("SP_TILE")
     base.autotune(3)
     assert 0 <= base.kernel_info()["variant"] < nv
+
+
+@pytest.mark.parametrize("dims,ybc", [((128, 40, 24), "periodic"), ((256, 36, 20), "periodic"),
+                                      ((128, 34, 18), "dirichlet")])
+def test_row_kernels_give_the_same_fields(dims, ybc, monkeypatch):
+    """The row kernels of the conserved pattern (whole x rows per CTA, x
+    neighbours by warp shuffles) run on grids of x extent 128 or 256,
+    periodic in x; on such grids they must give the bits of every other tile
+    shape -- here with ragged y tiles, and with Dirichlet y sides."""
+    P, D = sp.BoundaryType.PERIODIC, sp.BoundaryType.DEFAULT
+    bc = [P, P] + ([P, P] if ybc == "periodic" else [D, D]) + [P, P]
+
+    def make(cls):
+        return cls(3, sp.SolverFT(S3, form="fused"),
+                   sp.ProblemParameters(dims, h=1.0, boundary=bc, boundary_value=0.25),
+                   dtype="f32")
+
+    for cls in (sp.model_MB_t, sp.model_MBMK_t):
+        nv = make(cls).kernel_info()["variants"]
+        ref, rows = None, 0
+        for v in range(nv):
+            monkeypatch.setenv("SP_TILE", str(v))
+            m = make(cls)
+            info = m.kernel_info()
+            if info["variant"] != v:
+                m.close()
+                continue
+            rows += info["tile_x"] == dims[0]
+            m.fill_uniform(0, 77, -0.35, -0.05)
+            masses = m.step_mass(0.004, 30)
+            out = m.get_field(0)
+            if ref is None:
+                ref, ref_mass = out, masses[0]
+            else:
+                assert np.array_equal(out, ref), (cls.__name__, v)
+                assert abs(masses[0] - ref_mass) <= 1e-12 * abs(ref_mass)
+            m.close()
+        monkeypatch.delenv("SP_TILE")
+        assert rows >= 1, cls.__name__
