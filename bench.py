@@ -148,8 +148,8 @@ class B3D:
     dtype = "f32"
     bytes_per_site = 8  # one FP32 read and one FP32 write of the field per step
     flush_each_step = True
-    kernel = "fused model B step (k_fd3d / k_ch3d, the autotuned tile variant)"
-    traffic_file = os.path.join(ROOT, "profiles", "k_fd3d_modelB_256cube_f32.json")
+    kernel = "fused model B step (k_chrow / k_fd3d / k_ch3d, the autotuned tile variant)"
+    traffic_file = os.path.join(ROOT, "profiles", "k_chrow_modelB_256cube_f32.json")
     workload = ("Cahn-Hilliard (model B) 3D 256^3 periodic, dx 1, dt 0.005, "
                 "Stencil3d2h<7,10,25>, fused step, psi_bar -0.2 +- 0.1 seeded noise")
 
