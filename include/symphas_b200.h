@@ -91,6 +91,9 @@ typedef struct sp_desc {
   double coeff[8];      /* c(1)..c(8); unused entries should be 1 (c(i) default) */
   int ncoeff;
   int batch;            /* number of identical independent instances (>= 1) */
+  int accuracy;         /* order of accuracy of the stencils: 2 (or 0):
+                           Stencil2d2h / Stencil3d2h; 4: Stencil2d4h
+                           (sol/inc/stencilh4.h; 2D only) */
 } sp_desc;
 
 typedef struct sp_handle sp_handle;

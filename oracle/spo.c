@@ -69,6 +69,7 @@ typedef struct spo_desc {
   double c[8];      /* c(1)..c(8) */
   int bc[6];        /* sides in the order LEFT RIGHT TOP BOTTOM FRONT BACK */
   double bcv[6];    /* constant value of a DIRICHLET side */
+  int acc;          /* order of accuracy: 2 (or 0) Stencil2d2h/3d2h, 4 Stencil2d4h */
 } spo_desc;
 
 /* ------------------------------------------------------------------ */
@@ -269,14 +270,116 @@ static void spo_update_halo(const spo_desc* d, const spo_geom* g, double* v) {
 #define vx2_y2_z2 P(-2, -2, 2)
 #define vx2_y2_z2_ P(-2, -2, -2)
 
+#define vx3 P(3, 0, 0)
+#define vx3_ P(-3, 0, 0)
+#define vy3 P(0, 3, 0)
+#define vy3_ P(0, -3, 0)
+#define vx3y P(3, 1, 0)
+#define vx3y_ P(3, -1, 0)
+#define vx3_y P(-3, 1, 0)
+#define vx3_y_ P(-3, -1, 0)
+#define vxy3 P(1, 3, 0)
+#define vxy3_ P(1, -3, 0)
+#define vx_y3 P(-1, 3, 0)
+#define vx_y3_ P(-1, -3, 0)
+#define vx3y3 P(3, 3, 0)
+#define vx3y3_ P(3, -3, 0)
+#define vx3_y3 P(-3, 3, 0)
+#define vx3_y3_ P(-3, -3, 0)
+
 typedef struct {
   long sx, sy, sz;
   double divh2, divh3, divh4;
-  int lap, grad, bilap, dim;
+  int lap, grad, bilap, dim, acc;
 } spo_stencil;
+
+/* Stencil2d4h, sol/inc/stencilh4.h:44-216.  The reference hands every
+ * operator divh3 as its scale (sol/inc/stencilincludes.h:446, :453, :460),
+ * so s = divh3 below for the Laplacian and the bilaplacian too. */
+static double spo_lap4(const spo_stencil* st, const double* v) {
+  const long sx = st->sx, sy = st->sy, sz = 0;
+  const double s = st->divh3;
+  switch (st->lap) {
+    case 9:
+      return (-vx2_ - vx2 - vy2 - vy2_ + 16. * (vx_ + vx + vy + vy_) - 60. * v0) * s * (1.0 / 12);
+    case 17:
+      return (-(vx2y2 + vx2_y2 + vx2y2_ + vx2_y2_) - 8. * (vx2 + vx2_ + vy2 + vy2_) +
+              16. * (vxy + vx_y + vxy_ + vx_y_) + 128. * (vx + vx_ + vy + vy_) - 540. * v0) *
+             s * (1.0 / 120);
+    case 21:
+      return (-2. * (vx2y + vx2_y + vx2y_ + vx2_y_ + vxy2 + vx_y2 + vxy2_ + vx_y2_) -
+              (vx2 + vx2_ + vy2 + vy2_) + 16. * (vxy + vx_y + vxy_ + vx_y_) +
+              52. * (vx + vx_ + vy + vy_) - 252. * v0) *
+             s * (1.0 / 60);
+  }
+  abort();
+}
+
+static double spo_bilap4(const spo_stencil* st, const double* v) {
+  const long sx = st->sx, sy = st->sy, sz = 0;
+  const double s = st->divh3;
+  switch (st->bilap) {
+    case 21:
+      return (-4. * (vx3 + vx3_ + vy3 + vy3_) - (vx2y2 + vx2_y2 + vx2y2_ + vx2_y2_) +
+              50. * (vx2 + vx2_ + vy2 + vy2_) + 64. * (vxy + vx_y + vxy_ + vx_y_) -
+              284. * (vx + vx_ + vy + vy_) + 700. * v0) *
+             s * (1.0 / 24);
+    case 25:
+      return (-(vx3 + vx3_ + vy3 + vy3_) -
+              (vx2y + vx2_y + vx2y_ + vx2_y_ + vxy2 + vx_y2 + vxy2_ + vx_y2_) +
+              14. * (vx2 + vx2_ + vy2 + vy2_) + 20. * (vxy + vx_y + vxy_ + vx_y_) -
+              77. * (vx + vx_ + vy + vy_) + 184. * v0) *
+             s * (1.0 / 6);
+    case 33:
+      return (-17. * (vx3y3 + vx3_y3 + vx3y3_ + vx3_y3_) - 236. * (vx3 + vx3_ + vy3 + vy3_) +
+              351. * (vx2y2 + vx2_y2 + vx2y2_ + vx2_y2_) -
+              756. * (vx2y + vx2_y + vx2y_ + vx2_y_ + vxy2 + vx_y2 + vxy2_ + vx_y2_) +
+              4050. * (vx2 + vx2_ + vy2 + vy2_) + 5049. * (vxy + vx_y + vxy_ + vx_y_) -
+              19116. * (vx + vx_ + vy + vy_) + 45724. * v0) *
+             s * (1.0 / 1620);
+    case 37:
+      return (-17. * (vx3y + vx3_y + vx3y_ + vx3_y_ + vxy3 + vx_y3 + vxy3_ + vx_y3_) +
+              4. * (vx3 + vx3_ + vy3 + vy3_) - 29. * (vx2y2 + vx2_y2 + vx2y2_ + vx2_y2_) +
+              188. * (vx2y + vx2_y + vx2y_ + vx2_y_ + vxy2 + vx_y2 + vxy2_ + vx_y2_) +
+              42. * (vx2 + vx2_ + vy2 + vy2_) - 374. * (vxy + vx_y + vxy_ + vx_y_) -
+              764. * (vx + vx_ + vy + vy_) + 3116. * v0) *
+             s * (1.0 / 180);
+  }
+  abort();
+}
+
+static double spo_gradlap4_x(const spo_stencil* st, const double* v) {
+  const long sx = st->sx, sy = st->sy, sz = 0;
+  const double s = st->divh3;
+  switch (st->grad) {
+    case 14:
+      return (-6. * (vx3 - vx3_) - (vx2y2 - vx2_y2 + vx2y2_ - vx2_y2_) + 50. * (vx2 - vx2_) +
+              32. * (vxy - vx_y + vxy_ - vx_y_) - 142. * (vx - vx_)) *
+             s * (1.0 / 48);
+    case 18:
+      return (-3. * (vx3) - 2. * (vx2y - vx2_y + vx2y_ - vx2_y_) + 28. * (vx2) -
+              (vxy2 - vx_y2 + vxy2_ - vx_y2_) + 20. * (vxy - vx_y + vxy_ - vx_y_) - 77. * (vx)) *
+             s * (1.0 / 24);
+    case 26: /* the reference divides by 2160 divh3 here (stencilh4.h:184-195) */
+      return (-17. * (vx3y3 - vx3_y3 + vx3y3_ - vx3_y3_) - 236. * (vx3) +
+              234. * (vx2y2 - vx2_y2 + vx2y2_ - vx2_y2_) - 504. * (vx2y - vx2_y + vx2y_ - vx2_y_) +
+              2700. * (vx2) - 252. * (vxy2 - vx_y2 + vxy2_ - vx_y2_) +
+              1683. * (vxy - vx_y + vxy_ - vx_y_) - 6372. * (vx)) /
+             (2160. * s);
+    case 30:
+      return (-51. * (vx3y - vx3_y + vx3y_ - vx3_y_) + 12. * (vx3) -
+              58. * (vx2y2 - vx2_y2 + vx2y2_ - vx2_y2_) + 376. * (vx2y - vx2_y + vx2y_ - vx2_y_) +
+              84. * (vx2) - 17. * (vxy3 - vx_y3 + vxy3_ - vx_y3_) +
+              188. * (vxy2 - vx_y2 + vxy2_ - vx_y2_) - 374. * (vxy - vx_y + vxy_ - vx_y_) -
+              764. * (vx)) *
+             s * (1.0 / 720);
+  }
+  abort();
+}
 
 /* sol/inc/stencilh2.h:87-107 (2D) and :235-327 (3D) */
 static double spo_lap(const spo_stencil* st, const double* v) {
+  if (st->acc == 4) return spo_lap4(st, v);
   const long sx = st->sx, sy = st->sy, sz = st->sz;
   const double divh2 = st->divh2;
   if (st->dim == 2) {
@@ -316,6 +419,7 @@ static double spo_lap(const spo_stencil* st, const double* v) {
 
 /* sol/inc/stencilh2.h:112-156 (2D) and :329-412 (3D) */
 static double spo_bilap(const spo_stencil* st, const double* v) {
+  if (st->acc == 4) return spo_bilap4(st, v);
   const long sx = st->sx, sy = st->sy, sz = st->sz;
   const double divh4 = st->divh4;
   if (st->dim == 2) {
@@ -386,6 +490,7 @@ static double spo_bilap(const spo_stencil* st, const double* v) {
 
 /* x component of the gradlaplacian, sol/inc/stencilh2.h:161-221, :417-507 */
 static double spo_gradlap_x(const spo_stencil* st, const double* v) {
+  if (st->acc == 4) return spo_gradlap4_x(st, v);
   const long sx = st->sx, sy = st->sy, sz = st->sz;
   const double divh3 = st->divh3;
   if (st->dim == 2) {
@@ -481,6 +586,7 @@ static void spo_sys_init(spo_sys* s, const spo_desc* d, int threads) {
   s->st.grad = d->gradlap_pts;
   s->st.bilap = d->bilap_pts;
   s->st.dim = d->dim;
+  s->st.acc = d->acc == 4 ? 4 : 2;
   for (int f = 0; f < 2; ++f) {
     s->psi[f] = (double*)calloc(s->g.size, sizeof(double));
     s->dframe[f] = (double*)calloc(s->g.size, sizeof(double));

@@ -29,6 +29,7 @@ class Desc(ctypes.Structure):
         ("c", ctypes.c_double * 8),
         ("bc", ctypes.c_int * 6),
         ("bcv", ctypes.c_double * 6),
+        ("acc", ctypes.c_int),
     ]
 
 
@@ -60,7 +61,7 @@ def _load():
 _lib = _load()
 
 
-def make_desc(dim, n, model, h, dt, coeff=(), stencil=None, bc=PERIODIC, bcv=0.0):
+def make_desc(dim, n, model, h, dt, coeff=(), stencil=None, bc=PERIODIC, bcv=0.0, acc=2):
     d = Desc()
     d.dim = dim
     nn = list(n) + [1] * (3 - len(n))
@@ -70,6 +71,7 @@ def make_desc(dim, n, model, h, dt, coeff=(), stencil=None, bc=PERIODIC, bcv=0.0
     if stencil is None:
         stencil = (5, 6, 13) if dim == 2 else (7, 10, 25)
     d.lap_pts, d.gradlap_pts, d.bilap_pts = stencil
+    d.acc = acc
     d.h = h
     d.dt = dt
     cs = list(coeff) + [1.0] * (8 - len(coeff))

@@ -6,12 +6,12 @@ the fields stay resident in HBM.  The compute runs in lib/libsymphas_b200.so
 (C ABI in include/symphas_b200.h); this package is the host-side mirror.
 """
 from ._capi import SymPhasError, lib
-from .model import (BoundaryType, Ensemble, Model, ProblemParameters, SolverFT, Stencil2d2h,
+from .model import (BoundaryType, Ensemble, Model, ProblemParameters, SolverFT, Stencil2d2h, Stencil2d4h,
                     Stencil3d2h, ensemble_members, find_solution, model_MA_t, model_MAMK_t, model_MB_t, model_MBMK_t,
                     model_MC_t, model_OP_t)
 
 __all__ = [
-    "BoundaryType", "Ensemble", "Model", "ProblemParameters", "SolverFT", "Stencil2d2h", "Stencil3d2h",
+    "BoundaryType", "Ensemble", "Model", "ProblemParameters", "SolverFT", "Stencil2d2h", "Stencil2d4h", "Stencil3d2h",
     "SymPhasError", "ensemble_members", "find_solution", "lib", "model_MA_t", "model_MAMK_t", "model_MB_t",
     "model_MBMK_t", "model_MC_t", "model_OP_t",
 ]

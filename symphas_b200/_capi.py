@@ -54,6 +54,7 @@ class SpDesc(ctypes.Structure):
         ("coeff", ctypes.c_double * 8),
         ("ncoeff", ctypes.c_int),
         ("batch", ctypes.c_int),
+        ("accuracy", ctypes.c_int),
     ]
 
 

@@ -260,6 +260,10 @@ int validate(const sp_desc* d, std::string& why) {
   if (d->form != SP_FORM_EXACT && d->form != SP_FORM_FUSED) return why = "form must be exact or fused", SP_EINVAL;
   if (!(d->h > 0.0)) return why = "grid spacing h must be positive", SP_EINVAL;
   if (d->batch < 1) return why = "batch must be >= 1", SP_EINVAL;
+  if (d->accuracy != 0 && d->accuracy != 2 && d->accuracy != 4)
+    return why = "accuracy must be 2 (Stencil2d2h / Stencil3d2h) or 4 (Stencil2d4h)", SP_EINVAL;
+  if (d->accuracy == 4 && d->dim != 2)
+    return why = "4th-order stencils are two-dimensional (Stencil2d4h)", SP_EINVAL;
   for (int a = 0; a < d->dim; ++a) {
     const int l = d->boundary[2 * a], r = d->boundary[2 * a + 1];
     if ((l != SP_PERIODIC && l != SP_DIRICHLET) || (r != SP_PERIODIC && r != SP_DIRICHLET))
@@ -463,10 +467,13 @@ int configure(sp_handle* H, int variant) {
 std::mutex g_tune_mutex;
 std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int>, int> g_tuned;
 
+// the kernel-key code of a point count: 4th-order point sets are offset
+int pts_code(const sp_desc& d, int pts) { return d.accuracy == 4 ? sp::SP_PTS4 + pts : pts; }
+
 std::tuple<int, int, int, int, int, int, int, int, int, int, int> tune_key(const sp_handle* H) {
   const sp_desc& d = H->d;
-  return {d.model, d.form, d.dim, d.dtype, d.lap_pts, d.gradlap_pts, d.bilap_pts,
-          H->n[0], H->n[1], H->n[2], H->batch};
+  return {d.model, d.form, d.dim, d.dtype, pts_code(d, d.lap_pts), pts_code(d, d.gradlap_pts),
+          pts_code(d, d.bilap_pts), H->n[0], H->n[1], H->n[2], H->batch};
 }
 
 // kernel model of an ensemble: one model shared by every member, or the
@@ -519,14 +526,20 @@ int create(const sp_desc* desc, const sp_member* members, int count, sp_handle* 
   H->dim = dd.dim;
   H->batch = dd.batch;
   H->esz = dd.dtype == SP_F32 ? 4 : 8;
-  const sp::KernelKey key{dd.model, dd.form, dd.dim, dd.dtype,
-                          dd.lap_pts, dd.gradlap_pts, dd.bilap_pts};
+  const sp::KernelKey key{dd.model,
+                          dd.form,
+                          dd.dim,
+                          dd.dtype,
+                          pts_code(dd, dd.lap_pts),
+                          pts_code(dd, dd.gradlap_pts),
+                          pts_code(dd, dd.bilap_pts)};
   const std::vector<sp::KernelInfo>* vs = sp::find_kernels(key);
   if (!vs || vs->empty()) {
     char b[256];
     snprintf(b, sizeof b,
-             "no fused kernel built for model %d form %d dim %d dtype %d stencil <%d,%d,%d>",
-             dd.model, dd.form, dd.dim, dd.dtype, dd.lap_pts, dd.gradlap_pts, dd.bilap_pts);
+             "no fused kernel built for model %d form %d dim %d dtype %d stencil %dd%dh<%d,%d,%d>",
+             dd.model, dd.form, dd.dim, dd.dtype, dd.dim, dd.accuracy == 4 ? 4 : 2, dd.lap_pts,
+             dd.gradlap_pts, dd.bilap_pts);
     return fail(H, SP_EINVAL, b);
   }
   H->variants = *vs;

@@ -43,6 +43,7 @@ struct alignas(sizeof(T) * W) Vec {
 SP_VEC_BINOP(+)
 SP_VEC_BINOP(-)
 SP_VEC_BINOP(*)
+SP_VEC_BINOP(/)
 #undef SP_VEC_BINOP
 
 template <class T, int W>

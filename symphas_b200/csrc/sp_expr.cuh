@@ -159,47 +159,50 @@ __host__ __device__ constexpr StageRef<K> stage() {
 constexpr int rmax(int a, int b) { return a > b ? a : b; }
 constexpr int rplus(int a, int d) { return a < 0 ? -1 : a + d; }
 
-template <class E>
+// ACC: order of accuracy of the stencils (2: Stencil2d2h / Stencil3d2h, whose
+// Laplacians reach 1 and bilaplacians and gradlaplacians 2; 4: Stencil2d4h,
+// reaching 2, 3 and 3)
+template <class E, int ACC = 2>
 struct Reach {
   static constexpr int field = -1, stage = -1, max_var = 0, max_stage = -1;
 };
-template <int I>
-struct Reach<Var<I>> {
+template <int I, int ACC>
+struct Reach<Var<I>, ACC> {
   static constexpr int field = 0, stage = -1, max_var = I, max_stage = -1;
 };
-template <int K>
-struct Reach<StageRef<K>> {
+template <int K, int ACC>
+struct Reach<StageRef<K>, ACC> {
   static constexpr int field = -1, stage = 0, max_var = 0, max_stage = K;
 };
-template <class A, class B, template <class, class> class Op>
+template <class A, class B, int ACC>
 struct Reach2 {
-  static constexpr int field = rmax(Reach<A>::field, Reach<B>::field);
-  static constexpr int stage = rmax(Reach<A>::stage, Reach<B>::stage);
-  static constexpr int max_var = rmax(Reach<A>::max_var, Reach<B>::max_var);
-  static constexpr int max_stage = rmax(Reach<A>::max_stage, Reach<B>::max_stage);
+  static constexpr int field = rmax(Reach<A, ACC>::field, Reach<B, ACC>::field);
+  static constexpr int stage = rmax(Reach<A, ACC>::stage, Reach<B, ACC>::stage);
+  static constexpr int max_var = rmax(Reach<A, ACC>::max_var, Reach<B, ACC>::max_var);
+  static constexpr int max_stage = rmax(Reach<A, ACC>::max_stage, Reach<B, ACC>::max_stage);
 };
-template <class A, class B>
-struct Reach<Add<A, B>> : Reach2<A, B, Add> {};
-template <class A, class B>
-struct Reach<Sub<A, B>> : Reach2<A, B, Sub> {};
-template <class A, class B>
-struct Reach<Mul<A, B>> : Reach2<A, B, Mul> {};
-template <class A>
-struct Reach<Neg<A>> : Reach<A> {};
-template <int N, class A>
-struct Reach<Pow<N, A>> : Reach<A> {};
-template <class A, int D>
+template <class A, class B, int ACC>
+struct Reach<Add<A, B>, ACC> : Reach2<A, B, ACC> {};
+template <class A, class B, int ACC>
+struct Reach<Sub<A, B>, ACC> : Reach2<A, B, ACC> {};
+template <class A, class B, int ACC>
+struct Reach<Mul<A, B>, ACC> : Reach2<A, B, ACC> {};
+template <class A, int ACC>
+struct Reach<Neg<A>, ACC> : Reach<A, ACC> {};
+template <int N, class A, int ACC>
+struct Reach<Pow<N, A>, ACC> : Reach<A, ACC> {};
+template <class A, int D, int ACC>
 struct ReachD {
-  static constexpr int field = rplus(Reach<A>::field, D);
-  static constexpr int stage = rplus(Reach<A>::stage, D);
-  static constexpr int max_var = Reach<A>::max_var, max_stage = Reach<A>::max_stage;
+  static constexpr int field = rplus(Reach<A, ACC>::field, D);
+  static constexpr int stage = rplus(Reach<A, ACC>::stage, D);
+  static constexpr int max_var = Reach<A, ACC>::max_var, max_stage = Reach<A, ACC>::max_stage;
 };
-template <class A>
-struct Reach<Lap<A>> : ReachD<A, 1> {};
-template <class A>
-struct Reach<Bilap<A>> : ReachD<A, 2> {};
-template <class A>
-struct Reach<Gradlap<A>> : ReachD<A, 2> {};
+template <class A, int ACC>
+struct Reach<Lap<A>, ACC> : ReachD<A, ACC == 4 ? 2 : 1, ACC> {};
+template <class A, int ACC>
+struct Reach<Bilap<A>, ACC> : ReachD<A, ACC == 4 ? 3 : 2, ACC> {};
+template <class A, int ACC>
+struct Reach<Gradlap<A>, ACC> : ReachD<A, ACC == 4 ? 3 : 2, ACC> {};
 
 // ---------------------------------------------------------------------------
 // evaluation at offset (X,Y,Z) from the site a context points at.
@@ -408,7 +411,10 @@ struct Ev<Lap<A>> {
       const T sz = s.template at<0, 0, -1>() + s.template at<0, 0, 1>();
       return fmadd<true>(T(-6.0) * c.divh2, s.template at<0, 0, 0>(), ((sx + sy) + sz) * c.divh2);
     } else {
-      return st::lap_pts<C::dim, C::lap_points>::template apply<T>(s, c.divh2);
+      if constexpr (C::lap_points >= 1000)  // Stencil2d4h: scale divh3, as the reference
+        return st::lap4_pts<C::lap_points - 1000>::template apply<T>(s, c.divh3);
+      else
+        return st::lap_pts<C::dim, C::lap_points>::template apply<T>(s, c.divh2);
     }
   }
 };
@@ -418,7 +424,10 @@ struct Ev<Bilap<A>> {
   __device__ __forceinline__ static typename C::value_type at(const Bilap<A>& e, const C& c) {
     using T = typename C::value_type;
     Shifted<A, X, Y, Z, C> s{e.a, c};
-    return st::bilap_pts<C::dim, C::bilap_points>::template apply<T>(s, c.divh4);
+    if constexpr (C::bilap_points >= 1000)  // Stencil2d4h: scale divh3, as the reference
+      return st::bilap4_pts<C::bilap_points - 1000>::template apply<T>(s, c.divh3);
+    else
+      return st::bilap_pts<C::dim, C::bilap_points>::template apply<T>(s, c.divh4);
   }
 };
 template <class A>
@@ -427,7 +436,10 @@ struct Ev<Gradlap<A>> {
   __device__ __forceinline__ static typename C::value_type at(const Gradlap<A>& e, const C& c) {
     using T = typename C::value_type;
     Shifted<A, X, Y, Z, C> s{e.a, c};
-    return st::gradlap_pts<C::dim, C::gradlap_points>::template apply<T>(s, c.divh3);
+    if constexpr (C::gradlap_points >= 1000)
+      return st::gradlap4_pts<C::gradlap_points - 1000>::template apply<T>(s, c.divh3);
+    else
+      return st::gradlap_pts<C::dim, C::gradlap_points>::template apply<T>(s, c.divh3);
   }
 };
 
@@ -460,6 +472,26 @@ struct ModelDef {
   static_assert(Reach<R0>::max_var <= NF && Reach<R1>::max_var <= NF, "op(i) beyond the field count");
   static_assert(Reach<S0>::max_stage < 0 && Reach<S1>::max_stage < 0, "a staged operand may not use stages");
   static_assert(Reach<R0>::max_stage < NS && (NF < 2 || Reach<R1>::max_stage < NS), "stage index beyond NS");
+  // the same reaches for stencils of order of accuracy ACC
+  template <int ACC>
+  struct reach_at {
+    static constexpr int r_direct =
+        rmax(Reach<R0, ACC>::field, NF > 1 ? Reach<R1, ACC>::field : -1);
+    static constexpr int RS =
+        NS > 0 ? rmax(rmax(Reach<R0, ACC>::stage, NF > 1 ? Reach<R1, ACC>::stage : -1), 0) : 0;
+    static constexpr int r_stage =
+        rmax(NS > 0 ? Reach<S0, ACC>::field : -1, NS > 1 ? Reach<S1, ACC>::field : -1);
+    static constexpr int R = rmax(rmax(r_direct, NS > 0 ? RS + rmax(r_stage, 0) : 0), 0);
+  };
+};
+
+// A lowered model evaluated with stencils of order of accuracy ACC: the same
+// expressions, with the halo reaches of those stencils (the kernels read
+// R, RS, r_direct and r_stage from their model type)
+template <class M, int ACC>
+struct ModelAcc : M {
+  using RA = typename M::template reach_at<ACC>;
+  static constexpr int r_direct = RA::r_direct, RS = RA::RS, r_stage = RA::r_stage, R = RA::R;
 };
 
 template <int NF, int NS, class R0, class R1 = Lit, class S0 = Lit, class S1 = Lit>

@@ -49,8 +49,34 @@
   SP_REG3(SPK_OP_GRADLAP, SPK_EXACT, MF_OP_GRADLAP, T, DT, 7, 36, 25); \
   SP_REG3(SPK_OP_GRADLAP, SPK_EXACT, MF_OP_GRADLAP, T, DT, 7, 40, 25);
 
+// Stencil2d4h (2D, 4th order): the models with SymPhas's default point sets
+// Stencil2d4h<> = <9,14,21> (sol/inc/stencilincludes.h:774-779), and each
+// operator with every point set of sol/inc/stencilh4.h
+#define SP_EXACT_SET4(T, DT)                                                           \
+  SP_REG2(SPK_A, SPK_EXACT, MF4_A_exact, T, DT, 1009, 1014, 1021);                      \
+  SP_REG2(SPK_B, SPK_EXACT, MF4_B_exact, T, DT, 1009, 1014, 1021);                      \
+  SP_REG2(SPK_C, SPK_EXACT, MF4_C_exact, T, DT, 1009, 1014, 1021);                      \
+  SP_REG2(SPK_AMK, SPK_EXACT, MF4_AMK_exact, T, DT, 1009, 1014, 1021);                  \
+  SP_REG2(SPK_BMK, SPK_EXACT, MF4_BMK_exact, T, DT, 1009, 1014, 1021);                  \
+  SP_REG2(SPK_OP_LAPCUBE, SPK_EXACT, MF4_OP_LAPCUBE, T, DT, 1009, 1014, 1021);
+#define SP_OPS2_4(T, DT)                                                               \
+  SP_REG2(SPK_OP_LAP, SPK_EXACT, MF4_OP_LAP, T, DT, 1009, 1014, 1021);                  \
+  SP_REG2(SPK_OP_LAP, SPK_EXACT, MF4_OP_LAP, T, DT, 1017, 1014, 1021);                  \
+  SP_REG2(SPK_OP_LAP, SPK_EXACT, MF4_OP_LAP, T, DT, 1021, 1014, 1021);                  \
+  SP_REG2(SPK_OP_BILAP, SPK_EXACT, MF4_OP_BILAP, T, DT, 1009, 1014, 1021);              \
+  SP_REG2(SPK_OP_BILAP, SPK_EXACT, MF4_OP_BILAP, T, DT, 1009, 1014, 1025);              \
+  SP_REG2(SPK_OP_BILAP, SPK_EXACT, MF4_OP_BILAP, T, DT, 1009, 1014, 1033);              \
+  SP_REG2(SPK_OP_BILAP, SPK_EXACT, MF4_OP_BILAP, T, DT, 1009, 1014, 1037);              \
+  SP_REG2(SPK_OP_GRADLAP, SPK_EXACT, MF4_OP_GRADLAP, T, DT, 1009, 1014, 1021);          \
+  SP_REG2(SPK_OP_GRADLAP, SPK_EXACT, MF4_OP_GRADLAP, T, DT, 1009, 1018, 1021);          \
+  SP_REG2(SPK_OP_GRADLAP, SPK_EXACT, MF4_OP_GRADLAP, T, DT, 1009, 1026, 1021);          \
+  SP_REG2(SPK_OP_GRADLAP, SPK_EXACT, MF4_OP_GRADLAP, T, DT, 1009, 1030, 1021);
+
 namespace sp {
 void register_exact_kernels() {
+  SP_EXACT_SET4(double, 1)
+  SP_EXACT_SET4(float, 0)
+  SP_OPS2_4(double, 1)
   // the benchmarked point sets <5,6,13> / <7,10,25> and SymPhas's defaults (Stencil2d2h<> = <9,6,13>,
   // Stencil3d2h<> = <15,10,25>, sol/inc/stencilincludes.h:758-792, 884-921)
   SP_EXACT_SET(double, 1, 5, 6, 13, 7, 10, 25)

@@ -2,7 +2,8 @@
  * sp_inst_fused.cu -- kernels of the FUSED form (bilap = lap o lap, merged
  * derivatives, staged operands); FMA contraction allowed.  For point sets
  * where bilap is not lap o lap, the FUSED key runs the exact term order
- * compiled with FMA.
+ * compiled with FMA; so does every Stencil2d4h key (no 4th-order bilaplacian
+ * is a Laplacian applied twice).
  */
 #include "sp_launch.cuh"
 
@@ -23,7 +24,12 @@
   SP_REG2(SPK_C, SPK_FUSED, MF_C_exact, T, DT, 9, 6, 13);                            \
   SP_REG3(SPK_A, SPK_FUSED, MF_A_fused, T, DT, 15, 10, 25);                          \
   SP_REG3(SPK_B, SPK_FUSED, MF_B_exact, T, DT, 15, 10, 25);                          \
-  SP_REG3(SPK_C, SPK_FUSED, MF_C_exact, T, DT, 15, 10, 25);
+  SP_REG3(SPK_C, SPK_FUSED, MF_C_exact, T, DT, 15, 10, 25);                         \
+  SP_REG2(SPK_A, SPK_FUSED, MF4_A_exact, T, DT, 1009, 1014, 1021);                   \
+  SP_REG2(SPK_B, SPK_FUSED, MF4_B_exact, T, DT, 1009, 1014, 1021);                   \
+  SP_REG2(SPK_C, SPK_FUSED, MF4_C_exact, T, DT, 1009, 1014, 1021);                   \
+  SP_REG2(SPK_AMK, SPK_FUSED, MF4_AMK_exact, T, DT, 1009, 1014, 1021);               \
+  SP_REG2(SPK_BMK, SPK_FUSED, MF4_BMK_exact, T, DT, 1009, 1014, 1021);
 
 // extra tile shapes of the FP32 fused kernels, for sp_autotune
 #define SP_FUSED_VARIANTS3(MODEL, MF)                                                   \

@@ -151,6 +151,22 @@ SP_FACTORY(MF_OP_GRADLAP, models::op_gradlap())
 SP_FACTORY(MF_OP_LAPCUBE, models::op_lapcube())
 #undef SP_FACTORY
 
+// a model factory whose models carry the halo reaches of stencils of order of
+// accuracy ACC (Stencil2d4h: ACC = 4)
+template <class MF, int ACC>
+struct MFAcc {
+  constexpr auto operator()() const { return ex::ModelAcc<decltype(MF{}()), ACC>{MF{}()}; }
+};
+using MF4_A_exact = MFAcc<MF_A_exact, 4>;
+using MF4_B_exact = MFAcc<MF_B_exact, 4>;
+using MF4_C_exact = MFAcc<MF_C_exact, 4>;
+using MF4_AMK_exact = MFAcc<MF_AMK_exact, 4>;
+using MF4_BMK_exact = MFAcc<MF_BMK_exact, 4>;
+using MF4_OP_LAP = MFAcc<MF_OP_LAP, 4>;
+using MF4_OP_BILAP = MFAcc<MF_OP_BILAP, 4>;
+using MF4_OP_GRADLAP = MFAcc<MF_OP_GRADLAP, 4>;
+using MF4_OP_LAPCUBE = MFAcc<MF_OP_LAPCUBE, 4>;
+
 }  // namespace sp
 
 // model ids and forms, as in include/symphas_b200.h

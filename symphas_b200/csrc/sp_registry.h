@@ -20,6 +20,9 @@ namespace sp {
 struct KernelKey {
   int model, form, dim, dtype, lp, gp, bp;
 };
+// kernel keys carry a point set of a 4th-order stencil (Stencil2d4h) as
+// SP_PTS4 + points: its point counts overlap the 2nd-order ones (lap 9, bilap 21)
+constexpr int SP_PTS4 = 1000;
 
 struct KernelInfo {
   int nf;       // fields

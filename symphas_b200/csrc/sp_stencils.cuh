@@ -1,5 +1,6 @@
 /*
- * sp_stencils.cuh -- second-order finite-difference stencils on an accessor.
+ * sp_stencils.cuh -- second- and fourth-order finite-difference stencils on an
+ * accessor.
  *
  * Every point variant of SymPhas's 2nd-order stencils (sol/inc/stencilh2.h:
  * 2D :87-221, 3D :235-507), written with the summation order of the
@@ -124,6 +125,23 @@ namespace st {
 #define vx2_y2z2_ P(-2, 2, -2)
 #define vx2_y2_z2 P(-2, -2, 2)
 #define vx2_y2_z2_ P(-2, -2, -2)
+
+#define vx3 P(3, 0, 0)
+#define vx3_ P(-3, 0, 0)
+#define vy3 P(0, 3, 0)
+#define vy3_ P(0, -3, 0)
+#define vx3y P(3, 1, 0)
+#define vx3y_ P(3, -1, 0)
+#define vx3_y P(-3, 1, 0)
+#define vx3_y_ P(-3, -1, 0)
+#define vxy3 P(1, 3, 0)
+#define vxy3_ P(1, -3, 0)
+#define vx_y3 P(-1, 3, 0)
+#define vx_y3_ P(-1, -3, 0)
+#define vx3y3 P(3, 3, 0)
+#define vx3y3_ P(3, -3, 0)
+#define vx3_y3 P(-3, 3, 0)
+#define vx3_y3_ P(-3, -3, 0)
 
 template <int DIM, int N> struct lap_pts;
 template <> struct lap_pts<2, 5> {
@@ -275,6 +293,136 @@ template <> struct gradlap_pts<3, 40> {
   }
 };
 
+// ---------------------------------------------------------------------------
+// 4th-order 2D stencils (Stencil2d4h, sol/inc/stencilh4.h): every point set of
+// the reference, in its summation order.  The `s` argument is the scale
+// factor the reference passes: Stencil2d4h gives all three operators divh3
+// (sol/inc/stencilincludes.h:446, :453, :460), so the Laplacian and the
+// bilaplacian scale correctly only for h = 1; that behaviour is kept.
+// ---------------------------------------------------------------------------
+template <int N> struct lap4_pts;
+template <> struct lap4_pts<9> {  // stencilh4.h:44-53
+  template <class T, class A>
+  __device__ __forceinline__ static T apply(const A& a, T s) {
+    return (-vx2_ - vx2 - vy2 - vy2_ + K(16.) * (vx_ + vx + vy + vy_) - K(60.) * v0) * s * K(1.0 / 12);
+  }
+};
+template <> struct lap4_pts<17> {  // stencilh4.h:55-67
+  template <class T, class A>
+  __device__ __forceinline__ static T apply(const A& a, T s) {
+    return (-(vx2y2 + vx2_y2 + vx2y2_ + vx2_y2_) - K(8.) * (vx2 + vx2_ + vy2 + vy2_) +
+            K(16.) * (vxy + vx_y + vxy_ + vx_y_) + K(128.) * (vx + vx_ + vy + vy_) - K(540.) * v0) *
+           s * K(1.0 / 120);
+  }
+};
+template <> struct lap4_pts<21> {  // stencilh4.h:69-82
+  template <class T, class A>
+  __device__ __forceinline__ static T apply(const A& a, T s) {
+    return (-K(2.) * (vx2y + vx2_y + vx2y_ + vx2_y_ + vxy2 + vx_y2 + vxy2_ + vx_y2_) -
+            (vx2 + vx2_ + vy2 + vy2_) + K(16.) * (vxy + vx_y + vxy_ + vx_y_) +
+            K(52.) * (vx + vx_ + vy + vy_) - K(252.) * v0) *
+           s * K(1.0 / 60);
+  }
+};
+template <int N> struct bilap4_pts;
+template <> struct bilap4_pts<21> {  // stencilh4.h:85-98
+  template <class T, class A>
+  __device__ __forceinline__ static T apply(const A& a, T s) {
+    return (-K(4.) * (vx3 + vx3_ + vy3 + vy3_) - (vx2y2 + vx2_y2 + vx2y2_ + vx2_y2_) +
+            K(50.) * (vx2 + vx2_ + vy2 + vy2_) + K(64.) * (vxy + vx_y + vxy_ + vx_y_) -
+            K(284.) * (vx + vx_ + vy + vy_) + K(700.) * v0) *
+           s * K(1.0 / 24);
+  }
+};
+template <> struct bilap4_pts<25> {  // stencilh4.h:100-113
+  template <class T, class A>
+  __device__ __forceinline__ static T apply(const A& a, T s) {
+    return (-(vx3 + vx3_ + vy3 + vy3_) -
+            (vx2y + vx2_y + vx2y_ + vx2_y_ + vxy2 + vx_y2 + vxy2_ + vx_y2_) +
+            K(14.) * (vx2 + vx2_ + vy2 + vy2_) + K(20.) * (vxy + vx_y + vxy_ + vx_y_) -
+            K(77.) * (vx + vx_ + vy + vy_) + K(184.) * v0) *
+           s * K(1.0 / 6);
+  }
+};
+template <> struct bilap4_pts<33> {  // stencilh4.h:115-131
+  template <class T, class A>
+  __device__ __forceinline__ static T apply(const A& a, T s) {
+    return (-K(17.) * (vx3y3 + vx3_y3 + vx3y3_ + vx3_y3_) - K(236.) * (vx3 + vx3_ + vy3 + vy3_) +
+            K(351.) * (vx2y2 + vx2_y2 + vx2y2_ + vx2_y2_) -
+            K(756.) * (vx2y + vx2_y + vx2y_ + vx2_y_ + vxy2 + vx_y2 + vxy2_ + vx_y2_) +
+            K(4050.) * (vx2 + vx2_ + vy2 + vy2_) + K(5049.) * (vxy + vx_y + vxy_ + vx_y_) -
+            K(19116.) * (vx + vx_ + vy + vy_) + K(45724.) * v0) *
+           s * K(1.0 / 1620);
+  }
+};
+template <> struct bilap4_pts<37> {  // stencilh4.h:133-148
+  template <class T, class A>
+  __device__ __forceinline__ static T apply(const A& a, T s) {
+    return (-K(17.) * (vx3y + vx3_y + vx3y_ + vx3_y_ + vxy3 + vx_y3 + vxy3_ + vx_y3_) +
+            K(4.) * (vx3 + vx3_ + vy3 + vy3_) - K(29.) * (vx2y2 + vx2_y2 + vx2y2_ + vx2_y2_) +
+            K(188.) * (vx2y + vx2_y + vx2y_ + vx2_y_ + vxy2 + vx_y2 + vxy2_ + vx_y2_) +
+            K(42.) * (vx2 + vx2_ + vy2 + vy2_) - K(374.) * (vxy + vx_y + vxy_ + vx_y_) -
+            K(764.) * (vx + vx_ + vy + vy_) + K(3116.) * v0) *
+           s * K(1.0 / 180);
+  }
+};
+// gradlaplacians: the x component, as the reference returns
+template <int N> struct gradlap4_pts;
+template <> struct gradlap4_pts<14> {  // stencilh4.h:150-163
+  template <class T, class A>
+  __device__ __forceinline__ static T apply(const A& a, T s) {
+    return (-K(6.) * (vx3 - vx3_) - (vx2y2 - vx2_y2 + vx2y2_ - vx2_y2_) + K(50.) * (vx2 - vx2_) +
+            K(32.) * (vxy - vx_y + vxy_ - vx_y_) - K(142.) * (vx - vx_)) *
+           s * K(1.0 / 48);
+  }
+};
+template <> struct gradlap4_pts<18> {  // stencilh4.h:165-179
+  template <class T, class A>
+  __device__ __forceinline__ static T apply(const A& a, T s) {
+    return (-K(3.) * (vx3) - K(2.) * (vx2y - vx2_y + vx2y_ - vx2_y_) + K(28.) * (vx2) -
+            (vxy2 - vx_y2 + vxy2_ - vx_y2_) + K(20.) * (vxy - vx_y + vxy_ - vx_y_) - K(77.) * (vx)) *
+           s * K(1.0 / 24);
+  }
+};
+template <> struct gradlap4_pts<26> {  // stencilh4.h:181-197: divides by 2160 s
+  template <class T, class A>
+  __device__ __forceinline__ static T apply(const A& a, T s) {
+    return (-K(17.) * (vx3y3 - vx3_y3 + vx3y3_ - vx3_y3_) - K(236.) * (vx3) +
+            K(234.) * (vx2y2 - vx2_y2 + vx2y2_ - vx2_y2_) - K(504.) * (vx2y - vx2_y + vx2y_ - vx2_y_) +
+            K(2700.) * (vx2) - K(252.) * (vxy2 - vx_y2 + vxy2_ - vx_y2_) +
+            K(1683.) * (vxy - vx_y + vxy_ - vx_y_) - K(6372.) * (vx)) /
+           (K(2160.) * s);
+  }
+};
+template <> struct gradlap4_pts<30> {  // stencilh4.h:199-216
+  template <class T, class A>
+  __device__ __forceinline__ static T apply(const A& a, T s) {
+    return (-K(51.) * (vx3y - vx3_y + vx3y_ - vx3_y_) + K(12.) * (vx3) -
+            K(58.) * (vx2y2 - vx2_y2 + vx2y2_ - vx2_y2_) + K(376.) * (vx2y - vx2_y + vx2y_ - vx2_y_) +
+            K(84.) * (vx2) - K(17.) * (vxy3 - vx_y3 + vxy3_ - vx_y3_) +
+            K(188.) * (vxy2 - vx_y2 + vxy2_ - vx_y2_) - K(374.) * (vxy - vx_y + vxy_ - vx_y_) -
+            K(764.) * (vx)) *
+           s * K(1.0 / 720);
+  }
+};
+
+#undef vx3
+#undef vx3_
+#undef vy3
+#undef vy3_
+#undef vx3y
+#undef vx3y_
+#undef vx3_y
+#undef vx3_y_
+#undef vxy3
+#undef vxy3_
+#undef vx_y3
+#undef vx_y3_
+#undef vx3y3
+#undef vx3y3_
+#undef vx3_y3
+#undef vx3_y3_
+
 #undef P
 #undef v0
 #undef vx
@@ -377,6 +525,7 @@ template <> struct gradlap_pts<3, 40> {
 #undef vx2_y2z2_
 #undef vx2_y2_z2
 #undef vx2_y2_z2_
+
 #undef K
 
 // reach (Chebyshev radius) of each operator's point set

@@ -43,11 +43,17 @@ using namespace sp::ex;
 
 template <int L = 9, int G = 6, int B = 13>
 struct Stencil2d2h {
-  static constexpr int dim = 2, lp = L, gp = G, bp = B;
+  static constexpr int dim = 2, lp = L, gp = G, bp = B, acc = 2;
 };
 template <int L = 15, int G = 10, int B = 25>
 struct Stencil3d2h {
-  static constexpr int dim = 3, lp = L, gp = G, bp = B;
+  static constexpr int dim = 3, lp = L, gp = G, bp = B, acc = 2;
+};
+// 4th order of accuracy (sol/inc/stencilh4.h, defaults sol/inc/stencilincludes.h:774-779);
+// every operator scaled by 1/h^3, as the reference does
+template <int L = 9, int G = 14, int B = 21>
+struct Stencil2d4h {
+  static constexpr int dim = 2, lp = L, gp = G, bp = B, acc = 4;
 };
 
 // SolverFT<Stencil, Exact>: Exact = evaluate without FMA contraction (compile
@@ -99,14 +105,18 @@ int registered_id() {
     static_assert(Sp::dim == D, "stencil dimension differs from the model's");
     const int mid = next_model_id();
     const int dt = sizeof(T) == 8 ? SP_F64 : SP_F32;
-    const sp::KernelKey key{mid, Solver::exact ? SP_FORM_EXACT : SP_FORM_FUSED, D, dt, Sp::lp,
-                            Sp::gp, Sp::bp};
-    if constexpr (D == 3)
+    // 4th-order point sets are keyed (and evaluated) as SP_PTS4 + points
+    constexpr int off = Sp::acc == 4 ? sp::SP_PTS4 : 0;
+    const sp::KernelKey key{mid, Solver::exact ? SP_FORM_EXACT : SP_FORM_FUSED, D, dt,
+                            off + Sp::lp, off + Sp::gp, off + Sp::bp};
+    if constexpr (D == 3) {
       sp::register_kernel(key, sp::Entry3<MF, T, Sp::lp, Sp::gp, Sp::bp,
                                           typename sp::Tiles<T>::D3, Solver::exact>::info());
-    else
-      sp::register_kernel(key, sp::Entry2<MF, MF, T, Sp::lp, Sp::gp, Sp::bp,
+    } else {
+      using MFA = sp::MFAcc<MF, Sp::acc>;  // the halo reach of the stencils
+      sp::register_kernel(key, sp::Entry2<MFA, MFA, T, off + Sp::lp, off + Sp::gp, off + Sp::bp,
                                           typename sp::Tiles<T>::D2, Solver::exact>::info());
+    }
     return mid;
   }();
   return id;
@@ -135,6 +145,7 @@ class model_t {
     d.lap_pts = Sp::lp;
     d.gradlap_pts = Sp::gp;
     d.bilap_pts = Sp::bp;
+    d.accuracy = Sp::acc;
     for (int s = 0; s < 6; ++s) {
       d.boundary[s] = p.boundary[s];
       d.boundary_value[s] = p.boundary_value[s];

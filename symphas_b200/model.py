@@ -28,6 +28,7 @@ class Stencil2d2h:
     """Stencil2d2h<L, G, B>: laplacian, gradlaplacian and bilaplacian point counts."""
 
     dim = 2
+    accuracy = 2
 
     def __init__(self, L=9, G=6, B=13):
         self.points = (int(L), int(G), int(B))
@@ -37,8 +38,22 @@ class Stencil3d2h:
     """Stencil3d2h<L, G, B>."""
 
     dim = 3
+    accuracy = 2
 
     def __init__(self, L=15, G=10, B=25):
+        self.points = (int(L), int(G), int(B))
+
+
+class Stencil2d4h:
+    """Stencil2d4h<L, G, B>: the 2D stencils of 4th order of accuracy
+    (sol/inc/stencilh4.h; defaults Stencil2d4h<> = <9, 14, 21>).  As in the
+    reference, every operator is scaled by 1/h^3 (stencilincludes.h:446-460),
+    which is exact for the Laplacian and bilaplacian only at h = 1."""
+
+    dim = 2
+    accuracy = 4
+
+    def __init__(self, L=9, G=14, B=21):
         self.points = (int(L), int(G), int(B))
 
 
@@ -102,6 +117,7 @@ class Model:
         d.model = self.model_id
         d.form = C.SP_FORM_EXACT if solver.form == "exact" else C.SP_FORM_FUSED
         d.lap_pts, d.gradlap_pts, d.bilap_pts = solver.stencil.points
+        d.accuracy = solver.stencil.accuracy
         for i in range(6):
             d.boundary[i] = params.boundary[i]
             d.boundary_value[i] = params.boundary_value[i]
@@ -335,6 +351,7 @@ class Ensemble(Model):
         d.dtype = self.dtype_code
         d.form = C.SP_FORM_EXACT if solver.form == "exact" else C.SP_FORM_FUSED
         d.lap_pts, d.gradlap_pts, d.bilap_pts = solver.stencil.points
+        d.accuracy = solver.stencil.accuracy
         for i in range(6):
             d.boundary[i] = params.boundary[i]
             d.boundary_value[i] = params.boundary_value[i]

@@ -6,8 +6,9 @@
 //        the order of SymPhas's printed scheme V^2(psi) - psi^3 + psi, exact form
 //   mbb: SymPhas's MBB (modeldefinitions.h:150-155), model B through a
 //        provisional variable var(1) = -(c1 - 4 c2 psi^2) psi, fused form
+//   ma4: the same MA with SymPhas's 4th-order stencils Stencil2d4h<>, exact
 //
-//   user_model <ma|mbb> <out> <n> <h> <dt> <steps> <seed> <lo> <hi>
+//   user_model <ma|mbb|ma4> <out> <n> <h> <dt> <steps> <seed> <lo> <hi>
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -35,7 +36,7 @@ int run(M& m, const char* out, unsigned long long seed, double lo, double hi, do
 
 int main(int argc, char** argv) {
   if (argc != 10) {
-    std::fprintf(stderr, "usage: %s ma|mbb out n h dt steps seed lo hi\n", argv[0]);
+    std::fprintf(stderr, "usage: %s ma|mbb|ma4 out n h dt steps seed lo hi\n", argv[0]);
     return 2;
   }
   const std::string which = argv[1];
@@ -47,6 +48,11 @@ int main(int argc, char** argv) {
   if (which == "ma") {
     const double coeff[2] = {1.0, 1.0};
     model_t<MA, SolverFT<Stencil2d2h<5, 6, 13>, true>, 2> m(coeff, 2, params);
+    return run(m, argv[2], seed, lo, hi, dt, steps);
+  }
+  if (which == "ma4") {
+    const double coeff[2] = {1.0, 1.0};
+    model_t<MA, SolverFT<Stencil2d4h<>, true>, 2> m(coeff, 2, params);
     return run(m, argv[2], seed, lo, hi, dt, steps);
   }
   if (which == "mbb") {

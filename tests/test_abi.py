@@ -4,6 +4,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 import symphas_b200 as sp
 from symphas_b200 import _capi
 
@@ -42,6 +44,25 @@ def test_create_rejects_bad_description_without_gpu_work():
     rc = sp.lib().sp_create(ctypes.byref(d), ctypes.byref(h))
     assert rc == _capi.SP_EINVAL
     assert b"dim" in sp.lib().sp_create_error()
+
+
+def _valid_desc(dim):
+    d = _capi.SpDesc()
+    d.dim = dim
+    for a in range(3):
+        d.n[a] = 16
+    d.dtype, d.model, d.form = _capi.SP_F64, 0, 1
+    d.h, d.batch = 1.0, 1
+    return d
+
+
+@pytest.mark.parametrize("dim,acc,word", [(2, 3, b"accuracy"), (3, 4, b"two-dimensional")])
+def test_create_rejects_bad_stencil_accuracy_without_gpu_work(dim, acc, word):
+    d = _valid_desc(dim)
+    d.accuracy = acc  # checked before any device call
+    h = _capi._H()
+    assert sp.lib().sp_create(ctypes.byref(d), ctypes.byref(h)) == _capi.SP_EINVAL
+    assert word in sp.lib().sp_create_error()
 
 
 def test_struct_layouts_match_the_header(tmp_path):

@@ -46,3 +46,17 @@ def test_provisional_variable_model(tmp_path):
     ref = spo.run(spo.make_desc(2, (n, n), spo.MODEL_B, h, dt),
                   spo.seed_uniform(seed, lo, hi, n * n).reshape(n, n), steps)
     assert float(np.max(np.abs(got - ref)) / np.max(np.abs(ref))) <= 1e-10
+
+
+def test_user_model_with_fourth_order_stencils(tmp_path):
+    """The same user-written MA with Stencil2d4h<> (4th order): bit-identical
+    to the oracle's model A with those stencils."""
+    n, h, dt, steps, seed, lo, hi = 48, 1.0, 0.01, 400, 13, -0.1, 0.1
+    out = tmp_path / "psi.bin"
+    r = subprocess.run([EXE, "ma4", str(out), str(n), str(h), str(dt), str(steps), str(seed),
+                        str(lo), str(hi)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(out, dtype=np.float64).reshape(n, n)
+    ref = spo.run(spo.make_desc(2, (n, n), spo.MODEL_A, h, dt, stencil=(9, 14, 21), acc=4),
+                  spo.seed_uniform(seed, lo, hi, n * n).reshape(n, n), steps)
+    assert np.array_equal(got, ref)

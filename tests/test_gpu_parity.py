@@ -294,3 +294,70 @@ def test_row_kernels_give_the_same_fields(dims, ybc, monkeypatch):
             m.close()
         monkeypatch.delenv("SP_TILE")
         assert rows >= 1, cls.__name__
+
+
+# ---------------------------------------------------------------------------
+# Stencil2d4h (4th order, 2D): every point set of each operator, and the
+# models with the default point sets, against the oracle in FP64 (exact form)
+# ---------------------------------------------------------------------------
+OPS2_4 = [("lap", (9, 14, 21)), ("lap", (17, 14, 21)), ("lap", (21, 14, 21)),
+          ("bilap", (9, 14, 21)), ("bilap", (9, 14, 25)), ("bilap", (9, 14, 33)),
+          ("bilap", (9, 14, 37)), ("gradlap", (9, 14, 21)), ("gradlap", (9, 18, 21)),
+          ("gradlap", (9, 26, 21)), ("gradlap", (9, 30, 21))]
+
+
+@pytest.mark.parametrize("op,pts", OPS2_4)
+def test_operator_2d4h_every_point_set(op, pts):
+    dims, h = (40, 36), 0.7
+    m = sp.model_OP_t(op, 2, sp.SolverFT(sp.Stencil2d4h(*pts), form="exact"),
+                      sp.ProblemParameters(dims, h=h))
+    m.fill_uniform(0, 98, -1.0, 1.0)
+    got = m.eval_rhs(0)
+    x = oracle_init(98, -1.0, 1.0, m.shape)
+    ref = spo.rhs(spo.make_desc(2, dims, OPID[op], h, 0.0, stencil=pts, acc=4), x)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("cls,oid,coeff", [(sp.model_MA_t, spo.MODEL_A, ()),
+                                           (sp.model_MB_t, spo.MODEL_B, ()),
+                                           (sp.model_MAMK_t, spo.MODEL_AMK, (1.3, 0.7)),
+                                           (sp.model_MBMK_t, spo.MODEL_BMK, (1.3, 0.7))])
+@pytest.mark.parametrize("h,bc", [(1.0, sp.BoundaryType.PERIODIC), (0.8, sp.BoundaryType.DEFAULT)])
+def test_models_2d4h_bit_identical(cls, oid, coeff, h, bc):
+    dims, dt, steps, val = (46, 38), 0.002, 60, 0.05
+    m = cls(2, sp.SolverFT(sp.Stencil2d4h(), form="exact"),
+            sp.ProblemParameters(dims, h=h, boundary=bc, boundary_value=val), coeff=coeff,
+            dtype="f64")
+    m.fill_uniform(0, 8, -0.2, 0.2)
+    sp.find_solution(m, dt, steps)
+    obc = spo.PERIODIC if bc == sp.BoundaryType.PERIODIC else spo.DIRICHLET
+    ref = spo.run(spo.make_desc(2, dims, oid, h, dt, coeff=coeff, stencil=(9, 14, 21), bc=obc,
+                                bcv=val, acc=4), oracle_init(8, -0.2, 0.2, m.shape), steps)
+    assert np.array_equal(m.get_field(0), ref)
+
+
+def test_model_c_2d4h_bit_identical():
+    dims, h, dt, steps, gamma = (36, 40), 1.0, 0.002, 50, 0.5
+    m = sp.model_MC_t(2, sp.SolverFT(sp.Stencil2d4h(), form="exact"),
+                      sp.ProblemParameters(dims, h=h), coeff=(gamma,), dtype="f64")
+    m.fill_uniform(0, 1, 0.0, 0.2)
+    m.fill_uniform(1, 2, -0.1, 0.1)
+    sp.find_solution(m, dt, steps)
+    got = np.stack([m.get_field(0), m.get_field(1)])
+    x = np.stack([oracle_init(1, 0.0, 0.2, m.shape), oracle_init(2, -0.1, 0.1, m.shape)])
+    ref = spo.run(spo.make_desc(2, dims, spo.MODEL_C, h, dt, coeff=(gamma,), stencil=(9, 14, 21),
+                                acc=4), x, steps)
+    assert np.array_equal(got, ref)
+
+
+def test_f32_2d4h_against_f64_oracle():
+    """The FP32 fused key of Stencil2d4h (the reference's term order with
+    FMA contraction): within FP32 rounding of the FP64 oracle."""
+    dims, h, dt, steps = (64, 48), 1.0, 0.002, 200
+    m = sp.model_MB_t(2, sp.SolverFT(sp.Stencil2d4h(), form="fused"), sp.ProblemParameters(dims, h=h),
+                      dtype="f32")
+    m.fill_uniform(0, 4, -0.3, 0.1)
+    x = m.get_field(0).astype(np.float64)
+    sp.find_solution(m, dt, steps)
+    ref = spo.run(spo.make_desc(2, dims, spo.MODEL_B, h, dt, stencil=(9, 14, 21), acc=4), x, steps)
+    assert rel_linf(m.get_field(0).astype(np.float64), ref) < 2e-5
