@@ -32,8 +32,10 @@
 namespace sp {
 
 // QP: keep psi at z - 1 .. z + 1 of the warp's rows in a register queue
-// (else read them from the plane ring, which holds them anyway)
-template <class M, int NXR_, int YW_, int SPT_, int PD_, bool QP_ = true>
+// (else read them from the plane ring, which holds them anyway); MINB: CTAs
+// per SM the register allocation must leave room for (1: no constraint beyond
+// one CTA)
+template <class M, int NXR_, int YW_, int SPT_, int PD_, bool QP_ = true, int MINB_ = 1>
 struct ChRow {
   using T = float;
   static constexpr int NXR = NXR_, G = NXR_ / 128, YW = YW_, SPT = SPT_, PD = PD_;
@@ -51,6 +53,9 @@ struct ChRow {
       256 + sizeof(T) * (size_t(NSLOT) * PLANE + 2 * size_t(MPL));
   // the field layout of the tile kernels of the same key (their x halo)
   static constexpr int HXA = HaloGeom<T, 2, R, 1, RS, RI>::HXA;
+  static constexpr int MINB = MINB_;
+  static_assert(MINB >= 1 && size_t(MINB) * (SMEM + 1024) <= 227 * 1024,
+                "the CTAs asked for fit the shared memory of an SM");
   static_assert(NXR == 128 || NXR == 256, "rows of one warp, one or two chunks per lane");
   static_assert(TY >= 1 && SPT >= 1, "at least one output row");
   static_assert(NT <= 1024, "threads per CTA");
@@ -61,8 +66,7 @@ struct ChRow {
 };
 
 template <class M, class KC>
-__global__ void __launch_bounds__(KC::NT)
-    k_chrow(const __grid_constant__ StepParams<float> p, const __grid_constant__ M m) {
+__device__ __forceinline__ void chrow_step(const StepParams<float>& p, const M& m) {
   using T = float;
   using V = Vec<float, 4>;
   constexpr int NXR = KC::NXR, G = KC::G, SPT = KC::SPT, TY = KC::TY, PD = KC::PD,
@@ -76,7 +80,7 @@ __global__ void __launch_bounds__(KC::NT)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
   T* fbuf = reinterpret_cast<T*>(smem_raw + 256);
-  T* mbuf = fbuf + NSLOT * PLANE;  // mu planes, alternating by z parity
+  T* mbuf = fbuf + NSLOT * PLANE;  // two mu planes, written and read alternately
   __shared__ double red[32];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -177,36 +181,51 @@ __global__ void __launch_bounds__(KC::NT)
   // psi and mu at planes z - 1, z, z + 1 relative to the output plane
   V qpsi[QP ? 3 : 1][SPT][G], qmu[3][SPT][G];
   double msum = 0.0;
-  int zslot = 0;  // ring slot of plane zi
+  // per-plane state, advanced by one plane per iteration (no divisions, no
+  // recomputation from zi): psi planes zi .. zi + 2 in the ring, the mbarrier
+  // slot and phase of plane zi + 2, the mu planes written and read, and this
+  // thread's output rows in plane zi
+  // (element offsets into the shared arrays, so every access stays a
+  // shared-memory access with a base the compiler knows)
+  int o0 = 0, o1 = PLANE, o2 = 2 * PLANE;  // psi planes zi, zi+1, zi+2
+  int wslot = 2;
+  uint32_t wph = 0;
+  int ow = ((zi0 + 1) & 1) * MPL;  // mu(zi+1), written now
+  int orr = (zi0 & 1) * MPL;       // mu(zi), written last iteration
+  T* oz[SPT];
+#pragma unroll
+  for (int k = 0; k < SPT; ++k) oz[k] = orow[k] + (long long)(zi0 + p.h[2]) * p.plane;
+  const bool rhs_only = p.rhs_only != 0;
+  const bool zper = p.per[2] != 0;
+  const int rows = m0 * NXR + xl;  // this warp's first mu row (psi box row m0 + 1)
 
   auto body = [&](auto phase_tag, int zi) -> bool {
     constexpr int P = decltype(phase_tag)::value;
     constexpr int IM = P % 3, IC = (P + 1) % 3, IP = (P + 2) % 3;
-    const int qw = zi + R - (zb - R);  // plane zi + 2
     bool bad = false;
     if (zi == zi0) {
-      for (int q = 0; q <= qw; ++q) bad |= !tma::mbar_wait(&bars[q % NSLOT], (q / NSLOT) & 1);
+      for (int q = 0; q <= 2; ++q) bad |= !tma::mbar_wait(&bars[q], 0);
     } else {
-      bad = !tma::mbar_wait(&bars[wrap<NSLOT>(zslot, R)], (qw / NSLOT) & 1);
+      bad = !tma::mbar_wait(&bars[wslot], wph);
     }
-    const T* f0 = fbuf + zslot * PLANE;                  // psi(zi)
-    const T* f1 = fbuf + wrap<NSLOT>(zslot, 1) * PLANE;  // psi(zi+1)
-    const T* f2 = fbuf + wrap<NSLOT>(zslot, 2) * PLANE;  // psi(zi+2)
-    // psi at z = zi - 1 + j (j = 0, 1, 2) of row k: the queue, or the ring
-    V pz[3][SPT][G];
-    T* mw = mbuf + ((zi + 1) & 1) * MPL;                 // mu(zi+1), written now
-    const T* mr = mbuf + (zi & 1) * MPL;                 // mu(zi), written last iteration
+    // psi at z = zi - 1 + j (j = 0, 1, 2) of row k: the queue, or the ring;
     // psi box row b holds y = y0 - 2 + b: mu row m has its centre at b = m + 1
+    V pz[3][SPT][G];
+    const T* const f0 = fbuf + o0;
+    const T* const f1 = fbuf + o1;
+    const T* const f2 = fbuf + o2;
+    T* const mw = mbuf + ow;
+    const T* const mr = mbuf + orr;
     if constexpr (QP) {
       if (zi == zi0) {
 #pragma unroll
         for (int k = 0; k < SPT; ++k) {
-          ld_row(f0 + (m0 + k + 1) * NXR, qpsi[IM][k]);
-          ld_row(f1 + (m0 + k + 1) * NXR, qpsi[IC][k]);
+          ld_row(f0 + rows + (k + 1) * NXR - xl, qpsi[IM][k]);
+          ld_row(f1 + rows + (k + 1) * NXR - xl, qpsi[IC][k]);
         }
       }
 #pragma unroll
-      for (int k = 0; k < SPT; ++k) ld_row(f2 + (m0 + k + 1) * NXR, qpsi[IP][k]);
+      for (int k = 0; k < SPT; ++k) ld_row(f2 + rows + (k + 1) * NXR - xl, qpsi[IP][k]);
 #pragma unroll
       for (int k = 0; k < SPT; ++k)
 #pragma unroll
@@ -218,16 +237,16 @@ __global__ void __launch_bounds__(KC::NT)
     } else {
 #pragma unroll
       for (int k = 0; k < SPT; ++k) {
-        ld_row(f0 + (m0 + k + 1) * NXR, pz[0][k]);
-        ld_row(f1 + (m0 + k + 1) * NXR, pz[1][k]);
-        ld_row(f2 + (m0 + k + 1) * NXR, pz[2][k]);
+        ld_row(f0 + rows + (k + 1) * NXR - xl, pz[0][k]);
+        ld_row(f1 + rows + (k + 1) * NXR - xl, pz[1][k]);
+        ld_row(f2 + rows + (k + 1) * NXR - xl, pz[2][k]);
       }
     }
     // ---- mu at zi + 1 on this warp's rows
     {
       V above[G], below[G];
-      ld_row(f1 + m0 * NXR, above);
-      ld_row(f1 + (m0 + SPT + 1) * NXR, below);
+      ld_row(f1 + rows - xl, above);
+      ld_row(f1 + rows + (SPT + 1) * NXR - xl, below);
 #pragma unroll
       for (int k = 0; k < SPT; ++k) {
         V sx[G];
@@ -247,31 +266,32 @@ __global__ void __launch_bounds__(KC::NT)
           else
             mu = pw - l;
           qmu[IP][k][g] = mu;
-          *reinterpret_cast<V*>(mw + (m0 + k) * NXR + 128 * g + xl) = mu;
+          *reinterpret_cast<V*>(mw + rows + k * NXR + 128 * g) = mu;
         }
       }
     }
     // ---- output at z = zi: psi + dt * M * lap(mu)
     if (zi >= zb) {
-      const long long zoff = (long long)(zi + p.h[2]) * p.plane;
-      const long long zo = image_offset(p.per[2], zi, 1, p.n[2], R, p.plane);
-      const bool plain = zo == 0 && !yimg;  // warp-uniform
+      // periodic z images only on the planes within R of a z face
+      const bool zf = zper && (zi < R || zi >= p.n[2] - R);
+      const long long zo = zf ? image_offset(1, zi, 1, p.n[2], R, p.plane) : 0;
+      const bool plain = !zf && !yimg;  // warp-uniform
 #pragma unroll
       for (int k = 0; k < SPT; ++k) {
         const int o = m0 + k - 1;  // warp-uniform
         if (o < 0 || o >= TY) continue;
         V sx[G], up[G], dn[G];
         xsum_row(qmu[IC][k], sx);
-        if (k == 0) ld_row(mr + (m0 - 1) * NXR, up);
-        if (k == SPT - 1) ld_row(mr + (m0 + SPT) * NXR, dn);
+        if (k == 0) ld_row(mr + rows - NXR - xl, up);
+        if (k == SPT - 1) ld_row(mr + rows + SPT * NXR - xl, dn);
 #pragma unroll
         for (int g = 0; g < G; ++g) {
           const V sy = (k == 0 ? up[g] : qmu[IC][k - 1][g]) + (k == SPT - 1 ? dn[g] : qmu[IC][k + 1][g]);
           const V sz = qmu[IM][k][g] + qmu[IP][k][g];
           V r = lap7(sx[g], sy, sz, qmu[IC][k][g], m6divh2, divh2);
           if constexpr (RH::has_m) r = mob * r;
-          const V nv = p.rhs_only ? r : fmadd<true>(vdt, r, pz[0][k][g]);
-          T* const b = orow[k] + zoff + 128 * g;
+          const V nv = rhs_only ? r : fmadd<true>(vdt, r, pz[0][k][g]);
+          T* const b = oz[k] + 128 * g;
           if (plain) {
             st_if(b, nv, oin[k]);
             st_if(b + xo[g], nv, oin[k] && xo[g] != 0);
@@ -285,34 +305,60 @@ __global__ void __launch_bounds__(KC::NT)
     return !__syncthreads_or(bad);
   };
 
-  // zi0, zi0 + 1 are warm-up iterations (mu only); one barrier per plane
-  int phase = 0;
-  for (int zi = zi0; zi < ze; ++zi) {
+  // zi0, zi0 + 1 are warm-up iterations (mu only); one barrier per plane; the
+  // body is unrolled over the three phases of the register queues
+  int zi = zi0;
+  bool failed = false;
+  auto step = [&](auto phase_tag) -> bool {  // false: stop
+    if (zi >= ze) return false;
     const int qn = zi + R + PD - (zb - R);
     if (tid == 0 && zi > zi0 && qn < nplanes) issue(qn);
-    bool ok;
-    if (phase == 0)
-      ok = body(std::integral_constant<int, 0>{}, zi);
-    else if (phase == 1)
-      ok = body(std::integral_constant<int, 1>{}, zi);
-    else
-      ok = body(std::integral_constant<int, 2>{}, zi);
-    if (!ok) {
+    if (!body(phase_tag, zi)) {
       if (tid == 0) {
         atomicExch(p.err, KERR_TMA_TIMEOUT);
         tma::drain(bars, NSLOT, zi == zi0 ? 0 : zi + R - (zb - R),
                    min(zi == zi0 ? NSLOT - 1 : qn, nplanes - 1));
       }
-      return;
+      failed = true;
+      return false;
     }
-    phase = phase == 2 ? 0 : phase + 1;
-    zslot = wrap<NSLOT>(zslot, 1);
+    o0 = o1;
+    o1 = o2;
+    o2 = o2 + PLANE == NSLOT * PLANE ? 0 : o2 + PLANE;
+    if (++wslot == NSLOT) {
+      wslot = 0;
+      wph ^= 1u;
+    }
+    const int t = ow;
+    ow = orr;
+    orr = t;
+#pragma unroll
+    for (int k = 0; k < SPT; ++k) oz[k] += p.plane;
+    ++zi;
+    return true;
+  };
+  while (step(std::integral_constant<int, 0>{}) && step(std::integral_constant<int, 1>{}) &&
+         step(std::integral_constant<int, 2>{})) {
   }
+  if (failed) return;
   if (p.partial) {
     const double s = block_sum<NT>(msum, red);
     if (tid == 0)
       p.partial[(size_t(blockIdx.z) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
   }
+}
+
+// the kernel, with the occupancy hint only for shapes that ask for more than
+// one CTA per SM (a hint of one changes the compiler's register choices)
+template <class M, class KC>
+__global__ void __launch_bounds__(KC::NT)
+    k_chrow(const __grid_constant__ StepParams<float> p, const __grid_constant__ M m) {
+  chrow_step<M, KC>(p, m);
+}
+template <class M, class KC>
+__global__ void __launch_bounds__(KC::NT, KC::MINB)
+    k_chrow_occ(const __grid_constant__ StepParams<float> p, const __grid_constant__ M m) {
+  chrow_step<M, KC>(p, m);
 }
 
 }  // namespace sp

@@ -26,14 +26,17 @@ void register_wide_kernels() {
   SP_WIDE3(SPK_B, MF_B_fused)
   SP_WIDE3(SPK_C, MF_C_fused)
   // row kernels of the conserved pattern (x extent 256 or 128, periodic in x)
-  SP_REGCHROW(SPK_B, MF_B_fused, 256, 10, 1, 2, true);
-  SP_REGCHROW(SPK_B, MF_B_fused, 256, 10, 1, 2, false);
-  SP_REGCHROW(SPK_B, MF_B_fused, 256, 18, 1, 2, true);
-  SP_REGCHROW(SPK_B, MF_B_fused, 256, 6, 1, 2, false);
-  SP_REGCHROW(SPK_B, MF_B_fused, 128, 9, 2, 2, true);
-  SP_REGCHROW(SPK_B, MF_B_fused, 128, 18, 1, 2, true);
-  SP_REGCHROW(SPK_BMK, MF_BMK_fused, 256, 10, 1, 2, true);
-  SP_REGCHROW(SPK_BMK, MF_BMK_fused, 128, 9, 2, 2, true);
+  SP_REGCHROW(SPK_B, MF_B_fused, 256, 10, 1, 2, true, 2);
+  SP_REGCHROW(SPK_B, MF_B_fused, 256, 10, 1, 2, false, 2);
+  SP_REGCHROW(SPK_B, MF_B_fused, 256, 18, 1, 2, true, 1);
+  SP_REGCHROW(SPK_B, MF_B_fused, 256, 6, 1, 2, false, 1);
+  SP_REGCHROW(SPK_B, MF_B_fused, 256, 6, 1, 2, true, 1);
+  SP_REGCHROW(SPK_B, MF_B_fused, 256, 6, 1, 3, false, 1);
+  SP_REGCHROW(SPK_B, MF_B_fused, 256, 3, 2, 2, false, 1);
+  SP_REGCHROW(SPK_B, MF_B_fused, 128, 9, 2, 2, true, 1);
+  SP_REGCHROW(SPK_B, MF_B_fused, 128, 18, 1, 2, true, 1);
+  SP_REGCHROW(SPK_BMK, MF_BMK_fused, 256, 10, 1, 2, true, 2);
+  SP_REGCHROW(SPK_BMK, MF_BMK_fused, 128, 9, 2, 2, true, 1);
   SP_WIDE2(SPK_A, MF_A_fused, MF_A_fused)
   SP_WIDE2(SPK_B, MF_B_fused, MF_B_fused)
   SP_WIDE2(SPK_ENS_AB, MF_AMK_fused, MF_BMK_fused)

@@ -71,12 +71,18 @@ struct EntryCh3 {
 
 // the row kernel of the conserved pattern (sp_chrow.cuh): grids of x extent
 // NXR, periodic in x
-template <class MF, int NXR, int YW, int SPT, int PD, bool QP>
+template <class MF, int NXR, int YW, int SPT, int PD, bool QP, int MINB>
 struct EntryChRow {
   using M = model_of<MF>;
-  using K = ChRow<M, NXR, YW, SPT, PD, QP>;
+  using K = ChRow<M, NXR, YW, SPT, PD, QP, MINB>;
+  static constexpr auto kernel() {
+    if constexpr (MINB > 1)
+      return k_chrow_occ<M, K>;
+    else
+      return k_chrow<M, K>;
+  }
   static cudaError_t launch(const void* prm, dim3 grid, cudaStream_t s) {
-    auto kern = k_chrow<M, K>;
+    auto kern = kernel();
     static cudaError_t attr = cudaFuncSetAttribute(
         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
     if (attr != cudaSuccess) return attr;
@@ -85,7 +91,7 @@ struct EntryChRow {
     return cudaGetLastError();
   }
   static int occupancy() {
-    auto kern = k_chrow<M, K>;
+    auto kern = kernel();
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, K::NT, K::SMEM) != cudaSuccess)
@@ -226,9 +232,9 @@ template <> struct Tiles<double> {
 #define SP_REG3T(MODEL, FORM, MF, T, DT, LP, GP, BP, TILE)                  \
   ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 3, DT, LP, GP, BP},    \
                         ::sp::Entry3<::sp::MF, T, LP, GP, BP, TILE, FORM == SPK_EXACT>::info())
-#define SP_REGCHROW(MODEL, MF, NXR, YW, SPT, PD, QP)                            \
+#define SP_REGCHROW(MODEL, MF, NXR, YW, SPT, PD, QP, MINB)                      \
   ::sp::register_kernel(::sp::KernelKey{MODEL, SPK_FUSED, 3, 0, 7, 10, 25},      \
-                        ::sp::EntryChRow<::sp::MF, NXR, YW, SPT, PD, QP>::info())
+                        ::sp::EntryChRow<::sp::MF, NXR, YW, SPT, PD, QP, MINB>::info())
 #define SP_REGCH3(MODEL, MF, TILE)                                          \
   ::sp::register_kernel(::sp::KernelKey{MODEL, SPK_FUSED, 3, 0, 7, 10, 25},  \
                         ::sp::EntryCh3<::sp::MF, float, TILE>::info())
