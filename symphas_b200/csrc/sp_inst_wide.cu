@@ -5,7 +5,8 @@
  * and share their field layout, so they are further tile shapes for
  * sp_autotune (registered after the fused set, in their own translation unit
  * so that the build compiles them in parallel), together with the row kernels
- * of the conserved pattern (sp_chrow.cuh).
+ * of the conserved pattern (sp_chrow.cuh) and of any fused 7-point model
+ * (sp_row.cuh).
  */
 #include "sp_launch.cuh"
 
@@ -36,6 +37,14 @@ void register_wide_kernels() {
   SP_REGCHROW(SPK_B, MF_B_fused, 128, 9, 2, 2, true, 1);
   SP_REGCHROW(SPK_B, MF_B_fused, 128, 18, 1, 2, true, 1);
   SP_REGCHROW(SPK_BMK, MF_BMK_fused, 256, 10, 1, 2, true, 2);
+  // row kernels of any fused 7-point model (sp_row.cuh)
+  SP_REGROW(SPK_C, MF_C_fused, 256, 6, 1, 1);
+  SP_REGROW(SPK_C, MF_C_fused, 256, 6, 2, 1);
+  SP_REGROW(SPK_C, MF_C_fused, 256, 10, 1, 1);
+  SP_REGROW(SPK_C, MF_C_fused, 128, 10, 2, 1);
+  SP_REGROW(SPK_A, MF_A_fused, 256, 8, 2, 1);
+  SP_REGROW(SPK_A, MF_A_fused, 128, 16, 2, 1);
+  SP_REGROW(SPK_B, MF_B_fused, 256, 10, 2, 2);
   SP_REGCHROW(SPK_BMK, MF_BMK_fused, 128, 9, 2, 2, true, 1);
   SP_WIDE2(SPK_A, MF_A_fused, MF_A_fused)
   SP_WIDE2(SPK_B, MF_B_fused, MF_B_fused)

@@ -5,6 +5,7 @@
 
 #include "sp_ch.cuh"
 #include "sp_chrow.cuh"
+#include "sp_row.cuh"
 #include "sp_kernels.cuh"
 #include "sp_models.cuh"
 #include "sp_registry.h"
@@ -100,6 +101,44 @@ struct EntryChRow {
   }
   static KernelInfo info() {
     KernelInfo i{1, 1, K::R, K::HXA, K::TX, K::TY, K::SPT, K::PD, K::NT, K::SMEM,
+                 &launch, &occupancy};
+    i.box_hx = 0;
+    i.nx_only = NXR;
+    return i;
+  }
+};
+
+// the row kernel of the fused 7-point models (sp_row.cuh): grids of x extent
+// NXR, periodic in x
+template <class MF, int NXR, int YW, int PD, int MINB>
+struct EntryRow {
+  using M = model_of<MF>;
+  using K = RowCfg<M, NXR, YW, PD, MINB>;
+  static constexpr auto kernel() {
+    if constexpr (MINB > 1)
+      return k_row_occ<M, K>;
+    else
+      return k_row<M, K>;
+  }
+  static cudaError_t launch(const void* prm, dim3 grid, cudaStream_t s) {
+    auto kern = kernel();
+    static cudaError_t attr = cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
+    if (attr != cudaSuccess) return attr;
+    const M m = MF{}();
+    kern<<<grid, K::NT, K::SMEM, s>>>(*static_cast<const StepParams<float>*>(prm), m);
+    return cudaGetLastError();
+  }
+  static int occupancy() {
+    auto kern = kernel();
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, K::NT, K::SMEM) != cudaSuccess)
+      return 1;
+    return n > 0 ? n : 1;
+  }
+  static KernelInfo info() {
+    KernelInfo i{K::NF, K::NS, K::R, K::HXA, K::TX, K::TY, K::SPT, K::PD, K::NT, K::SMEM,
                  &launch, &occupancy};
     i.box_hx = 0;
     i.nx_only = NXR;
@@ -235,6 +274,9 @@ template <> struct Tiles<double> {
 #define SP_REGCHROW(MODEL, MF, NXR, YW, SPT, PD, QP, MINB)                      \
   ::sp::register_kernel(::sp::KernelKey{MODEL, SPK_FUSED, 3, 0, 7, 10, 25},      \
                         ::sp::EntryChRow<::sp::MF, NXR, YW, SPT, PD, QP, MINB>::info())
+#define SP_REGROW(MODEL, MF, NXR, YW, PD, MINB)                                 \
+  ::sp::register_kernel(::sp::KernelKey{MODEL, SPK_FUSED, 3, 0, 7, 10, 25},      \
+                        ::sp::EntryRow<::sp::MF, NXR, YW, PD, MINB>::info())
 #define SP_REGCH3(MODEL, MF, TILE)                                          \
   ::sp::register_kernel(::sp::KernelKey{MODEL, SPK_FUSED, 3, 0, 7, 10, 25},  \
                         ::sp::EntryCh3<::sp::MF, float, TILE>::info())

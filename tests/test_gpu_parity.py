@@ -259,20 +259,23 @@ def test_every_tile_shape_gives_the_same_fields(dim, n, cls, monkeypatch):
 
 @pytest.mark.parametrize("dims,ybc", [((128, 40, 24), "periodic"), ((256, 36, 20), "periodic"),
                                       ((128, 34, 18), "dirichlet")])
-def test_row_kernels_give_the_same_fields(dims, ybc, monkeypatch):
-    """The row kernels of the conserved pattern (whole x rows per CTA, x
-    neighbours by warp shuffles) run on grids of x extent 128 or 256,
-    periodic in x; on such grids they must give the bits of every other tile
-    shape -- here with ragged y tiles, and with Dirichlet y sides."""
+@pytest.mark.parametrize("classes", [(sp.model_MB_t, sp.model_MBMK_t), (sp.model_MA_t,),
+                                     (sp.model_MC_t,)])
+def test_row_kernels_give_the_same_fields(dims, ybc, classes, monkeypatch):
+    """The row kernels (whole x rows per CTA, x neighbours by warp shuffles:
+    the conserved-pattern kernel for models B and BMK, the generic one for
+    every fused 7-point model) run on grids of x extent 128 or 256, periodic
+    in x; on such grids they must give the bits of every other tile shape --
+    here with ragged y tiles, and with Dirichlet y sides."""
     P, D = sp.BoundaryType.PERIODIC, sp.BoundaryType.DEFAULT
     bc = [P, P] + ([P, P] if ybc == "periodic" else [D, D]) + [P, P]
 
     def make(cls):
         return cls(3, sp.SolverFT(S3, form="fused"),
                    sp.ProblemParameters(dims, h=1.0, boundary=bc, boundary_value=0.25),
-                   dtype="f32")
+                   coeff=(0.5,) if cls is sp.model_MC_t else (), dtype="f32")
 
-    for cls in (sp.model_MB_t, sp.model_MBMK_t):
+    for cls in classes:
         nv = make(cls).kernel_info()["variants"]
         ref, rows = None, 0
         for v in range(nv):
@@ -283,9 +286,10 @@ def test_row_kernels_give_the_same_fields(dims, ybc, monkeypatch):
                 m.close()
                 continue
             rows += info["tile_x"] == dims[0]
-            m.fill_uniform(0, 77, -0.35, -0.05)
+            for f in range(cls.nfields):
+                m.fill_uniform(f, 77 + f, -0.35, -0.05)
             masses = m.step_mass(0.004, 30)
-            out = m.get_field(0)
+            out = np.stack([m.get_field(f) for f in range(cls.nfields)])
             if ref is None:
                 ref, ref_mass = out, masses[0]
             else:
