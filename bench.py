@@ -188,7 +188,7 @@ class C3D(B3D):
     bytes_per_site = 16  # two fields, each read and written once per step
     flush_each_step = False
     kernel = "fused model C step (k_row / k_fd3d, two fields, the autotuned tile variant)"
-    traffic_file = os.path.join(ROOT, "profiles", "k_fd3d_modelC_8x256cube_f32.json")
+    traffic_file = os.path.join(ROOT, "profiles", "k_row_modelC_8x256cube_f32.json")
     workload = ("model C (gamma 0.5) 3D, 8 instances of 256^3 periodic, dx 1, dt 0.005, "
                 "Stencil3d2h<7,10,25>, fused step, psi 0.1 +- 0.1, eta +- 0.1 seeded noise")
 
