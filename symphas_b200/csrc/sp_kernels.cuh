@@ -825,8 +825,30 @@ __global__ void __launch_bounds__(TC::NT)
   int xsr[K::NX1], xsc[K::NX1];
   extra_cells<NE, NT, K::NX, TY, RS, SWC, XC, TXT>(tid, xsr, xsc);
 
+  // When every CTA has many items (ensembles), they are taken from the queue
+  // in batches of 4, one batch requested ahead (thread 0 only): the atomic's
+  // result is needed a batch later, so its round trip to L2 stays off the path
+  // of the tile loop, and the one counter sees a quarter of the atomics.
+  // Batches never overlap, so a CTA that finds an item past the end holds no
+  // valid item in its next batch.  With few items per CTA, batches and items
+  // held ahead would unbalance the tail: those launches take one item at a
+  // time, when they need it.
+  const bool many = p.nitems >= 64 * int(gridDim.x);
+  constexpr int QB = 4;
+  int qcur = 0, qend = 0, qnext = 0;
+  if (tid == 0 && many) qnext = atomicAdd(&p.ctr[0], QB);
   auto fetch = [&]() -> int2 {
-    const int t = atomicAdd(&p.ctr[0], 1);
+    if (qcur == qend) {
+      if (many) {
+        qcur = qnext;
+        qend = qnext + QB;
+        qnext = atomicAdd(&p.ctr[0], QB);
+      } else {
+        qcur = atomicAdd(&p.ctr[0], 1);
+        qend = qcur + 1;
+      }
+    }
+    const int t = qcur++;
     if (t >= p.nitems) return make_int2(-1, 0);
     return p.items ? p.items[t] : make_int2(0, t);
   };
