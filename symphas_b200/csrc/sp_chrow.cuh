@@ -16,14 +16,13 @@
  * contiguous across the warp.  The x neighbours of a row are exchanged by warp
  * shuffles (periodic: the row wraps around the warp), so no x halo is loaded,
  * staged or computed; the CTA's mu rows (YW * SPT of them) cover its TY output
- * rows and
- * the rows above and below, so the mu ring of the tile kernels is just two
- * more rows of the same loop; the z neighbours of psi and mu live in register
- * queues.  Shared memory holds the TMA ring of psi planes (n_x x (TY + 4)
- * boxes, no x halo) and two mu planes, from which only the rows at warp
- * boundaries are read back, one iteration later, behind the single barrier per
- * plane.  Periodic images are stored as by the other
- * kernels (the fields keep their halo for every other consumer).
+ * rows and the rows above and below, so the mu ring of the tile kernels is
+ * just two more rows of the same loop; the z neighbours of psi and mu live in
+ * register queues.  Shared memory holds the TMA ring of psi planes
+ * (n_x x (TY + 4) boxes, no x halo) and two mu planes, from which only the
+ * rows at warp boundaries are read back, one iteration later, behind the
+ * single barrier per plane.  Periodic images are stored as by the other
+ * kernels, so the fields keep their halo for every other consumer.
  */
 #pragma once
 
