@@ -365,3 +365,37 @@ def test_f32_2d4h_against_f64_oracle():
     sp.find_solution(m, dt, steps)
     ref = spo.run(spo.make_desc(2, dims, spo.MODEL_B, h, dt, stencil=(9, 14, 21), acc=4), x, steps)
     assert rel_linf(m.get_field(0).astype(np.float64), ref) < 2e-5
+
+
+@pytest.mark.parametrize("cls", [sp.model_MB_t, sp.model_MC_t])
+def test_row_kernels_on_a_batch_of_instances(cls, monkeypatch):
+    """A batch of instances (one launch, instance = grid z index) on the row
+    kernels gives, instance by instance, the bits of the tile kernel."""
+    dims, batch = (128, 20, 12), 3
+    coeff = (0.5,) if cls is sp.model_MC_t else ()
+
+    def run(v):
+        monkeypatch.setenv("SP_TILE", str(v))
+        m = cls(3, sp.SolverFT(S3, form="fused"), sp.ProblemParameters(dims, h=1.0),
+                coeff=coeff, dtype="f32", batch=batch)
+        got_v = m.kernel_info()["variant"]
+        for i in range(batch):
+            for f in range(cls.nfields):
+                m.fill_uniform(f, 100 * i + f, -0.3, 0.1, inst=i)
+        m.step(0.004, 20)
+        out = np.stack([m.get_field(f, inst=i) for i in range(batch) for f in range(cls.nfields)])
+        m.close()
+        return got_v, out
+
+    _, ref = run(0)
+    nv = cls(3, sp.SolverFT(S3, form="fused"), sp.ProblemParameters(dims, h=1.0), coeff=coeff,
+             dtype="f32").kernel_info()["variants"]
+    rows = 0
+    for v in range(1, nv):
+        got_v, out = run(v)
+        if got_v != v:
+            continue
+        assert np.array_equal(out, ref), v
+        rows += 1
+    monkeypatch.delenv("SP_TILE")
+    assert rows >= 1
