@@ -286,6 +286,24 @@ class Ens:
 WORKLOADS = {"b3d": B3D, "c3d": C3D, "ensemble": Ens}
 
 
+def max_over_ranks(ms, dist, device="cuda"):
+    """The job's time: the slowest rank's (every rank gets it).  `dist` is
+    torch.distributed when the job has more than one rank, else None."""
+    if not dist:
+        return float(ms)
+    import torch
+
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, steps, sites, ms):
+    """Site-updates per second of the whole job: every rank advances its own
+    replica of `sites` sites by `steps` steps in `ms` milliseconds."""
+    return world * steps * sites / (ms * 1e-3)
+
+
 def cpu_rate(W, seconds, threads):
     """Site-updates/s of the CPU restatement (oracle) on the workload, FP64."""
     step, sites, close, what = W.cpu_system(threads)
@@ -392,11 +410,8 @@ def run_ours(args):
         dist.barrier()
     clk = clocks.stop()
     launches = w.model.launch_count() - launches0
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    job_ms = float(t.item())
-    value = world * args.steps * sites / (job_ms * 1e-3)
+    job_ms = max_over_ranks(total_ms, dist)
+    value = job_rate(world, args.steps, sites, job_ms)
     launch_ms = total_ms / args.steps
 
     # end to end through the public API: every field of the step's input from
@@ -435,11 +450,8 @@ def run_ours(args):
         download(host_out)
     e_end.record(stream)
     torch.cuda.synchronize()
-    t = torch.tensor([e_start.elapsed_time(e_end)], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_ms = float(t.item()) / e2e_calls
-    e2e_value = world * args.e2e_inner * sites / (e2e_ms * 1e-3)
+    e2e_ms = max_over_ranks(e_start.elapsed_time(e_end), dist) / e2e_calls
+    e2e_value = job_rate(world, args.e2e_inner, sites, e2e_ms)
     w.model.close()
 
     if rank != 0:
