@@ -160,3 +160,54 @@ def test_generated_sweep_runs_and_stays_bounded():
         if m["model"] == "BMK":
             assert abs(ens.reduce(0, inst=i)[0] - m0[i]) <= 1e-3 * f.size ** 0.5
     ens.close()
+
+
+def test_every_tile_shape_gives_the_same_members(monkeypatch):
+    """The autotuner may pick any tile shape of the ensemble kernel (2 or 4
+    sites per thread): each gives the same bits, ragged members included."""
+    members = with_dt(MEMBERS)
+    ref, nv = None, None
+    for v in range(64):
+        monkeypatch.setenv("SP_TILE", str(v))
+        ens = sp.Ensemble(sp.SolverFT(S2, form="fused"), members, dtype="f32")
+        info = ens.kernel_info()
+        nv = info["variants"]
+        if info["variant"] != v:
+            ens.close()
+            if v >= nv:
+                break
+            continue
+        seeded(ens, members)
+        ens.step(30)
+        out = [ens.get_field(0, inst=i) for i in range(len(members))]
+        ens.close()
+        if ref is None:
+            ref = out
+        else:
+            for a, b in zip(out, ref):
+                assert np.array_equal(a, b), v
+    monkeypatch.delenv("SP_TILE")
+    assert nv and nv > 1
+
+
+def test_large_ensemble_members_equal_the_systems_alone():
+    """72 members of 1024^2 (~37 K tiles): enough work per CTA that the
+    kernel takes its work items in batches, requested ahead.  Members must
+    still evolve exactly as the same systems run alone."""
+    base = {"dims": (1024, 1024), "model": "BMK", "coeff": (1.0, 1.0)}
+    members = with_dt([dict(base, model="AMK" if i % 2 else "BMK", coeff=(1.0 + 0.01 * i, 1.0))
+                       for i in range(72)])
+    ens = sp.Ensemble(sp.SolverFT(S2, form="fused"), members, dtype="f32")
+    for i in range(len(members)):
+        ens.fill_uniform(0, 500 + i, -0.3, 0.3, inst=i)
+    ens.step(3)
+    for i in (0, 35, 71):
+        m = members[i]
+        cls = sp.model_MAMK_t if m["model"] == "AMK" else sp.model_MBMK_t
+        alone = cls(2, sp.SolverFT(S2, form="fused"), sp.ProblemParameters(m["dims"]),
+                    coeff=m["coeff"], dtype="f32")
+        alone.fill_uniform(0, 500 + i, -0.3, 0.3)
+        alone.step(m["dt"], 3)
+        assert np.array_equal(ens.get_field(0, inst=i), alone.get_field(0)), i
+        alone.close()
+    ens.close()

@@ -298,6 +298,15 @@ def test_row_kernels_give_the_same_fields(dims, ybc, classes, monkeypatch):
             m.close()
         monkeypatch.delenv("SP_TILE")
         assert rows >= 1, cls.__name__
+        # the autotuner's timing launches (right-hand sides only, the row
+        # kernels among them) leave the model's state as it was
+        m = make(cls)
+        for f in range(cls.nfields):
+            m.fill_uniform(f, 77 + f, -0.35, -0.05)
+        m.autotune(2)
+        m.step_mass(0.004, 30)
+        assert np.array_equal(np.stack([m.get_field(f) for f in range(cls.nfields)]), ref)
+        m.close()
 
 
 # ---------------------------------------------------------------------------
