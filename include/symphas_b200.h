@@ -271,6 +271,67 @@ int sp_reduce_fields_noalloc(const void* fields, int dtype, int dim, const int n
 /* Message of the last failure of sp_reduce_fields_noalloc on this thread. */
 const char* sp_noalloc_error(void);
 
+/* ---- regional systems (moving window) ---------------------------------------
+ * SolverFT on SolverSystemFDwSD (sol/inc/solversystem.h:62-77): the system's
+ * RegionalGrid (datatypes/inc/grid.h:2038-2158) holds only a window of the
+ * domain -- select_region origin and dims in storage coordinates, each with a
+ * 3-deep rim -- and reads `empty` everywhere else; the solver evaluates the
+ * window's interior only, and update_regional_system
+ * (sol/inc/boundarysystem.h:438-471) moves the window after the field.
+ * Here the window is a handle of its own, stepped by the fused kernels: its
+ * halo is the rim, holding `empty` (constant) except along an axis that the
+ * window spans from origin 0, which stays periodic.  The domain itself must
+ * be periodic on every side; single-field models only (SymPhas gives every
+ * field of a multi-field model a window of its own).  Searches for the next
+ * window run on the host over a byte mask (value >= cutoff) that a kernel
+ * builds from the window, in the reference's buffer order. */
+typedef struct sp_regional_params {
+  double resize_delta;   /* time between window updates (params::regional_resize_time, 3.0) */
+  double padding_factor; /* window / bounding box (params::regional_resize_factor, 2.0) */
+  double cutoff_eps;     /* cutoff = minimum + eps (params::regional_resize_cutoff_eps, 1e-6) */
+  int fixed;             /* 1: re-centre keeping the size (params::regional_resize_is_fixed);
+                            0: resize to the bounding box again */
+} sp_regional_params;
+
+typedef struct sp_regional sp_regional;
+
+/* Create a regional system over the whole domain `desc` (dim 2 or 3, batch 1,
+ * periodic sides, a single-field model).  The window starts as the whole
+ * domain with empty = 0 (REGIONAL_GRID_OUTER_VALUE, grid.h:2022); the first
+ * update (the first step) resizes it around the values >= min + eps. */
+int sp_regional_create(const sp_desc* desc, const sp_regional_params* params,
+                       sp_regional** out);
+/* Whole-domain interior values (x-fastest, dtype of desc) in: the window
+ * takes the values at its cells. */
+int sp_regional_upload(sp_regional* r, const void* host, size_t bytes);
+/* Whole-domain interior values out: the window's interior, `empty` elsewhere. */
+int sp_regional_download(sp_regional* r, void* host, size_t bytes);
+/* `nsteps` iterations of run_model (modules-models.h:480-491): update(time)
+ * -- the window check -- then equation and step, then time += dt; the steps
+ * between window checks run as one sp_step of the window's handle. */
+int sp_regional_step(sp_regional* r, int nsteps);
+/* Move the window to origin / dims (RegionalGrid::adjust(select_region),
+ * grid.h:2118-2128), dims including the rim, each at most the domain's
+ * storage extent. */
+int sp_regional_adjust(sp_regional* r, const int origin[3], const int dims[3]);
+/* Origin and dims of the window; state = {empty, cutoff, time, next update
+ * index}. */
+int sp_regional_window(const sp_regional* r, int origin[3], int dims[3], double state[4]);
+/* The window's handle (null while the window has no interior): for
+ * sp_kernel_info, sp_launch_count, sp_set_stream and the like. */
+sp_handle* sp_regional_handle(sp_regional* r);
+const char* sp_regional_error(const sp_regional* r);
+void sp_regional_destroy(sp_regional* r);
+/* The window search alone, on the host (no GPU needed): the window after a
+ * re-centre (mode 0, grid::adjust_region) or a resize (mode 1,
+ * grid::resize_adjust_region with `factor` and `rel_eps`) of the window
+ * (origin, dims) of a domain with storage extents G, given the byte mask of
+ * the window's buffer (dims[0]*dims[1]*dims[2] bytes, x-fastest, rim
+ * included, nonzero where value >= cutoff). */
+int sp_region_search(int dim, const int G[3], const int origin[3], const int dims[3],
+                     const unsigned char* mask, int mode, double factor, double rel_eps,
+                     int new_origin[3], int new_dims[3]);
+
 const char* sp_last_error(const sp_handle* h);
 /* Message of the last failure of sp_create (no handle exists then). */
 const char* sp_create_error(void);

@@ -776,3 +776,560 @@ int spo_omp_max_threads(void) {
   return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------ */
+/* regional systems: the moving window of SolverSystemFDwSD            */
+/* ------------------------------------------------------------------ */
+/*
+ * A RegionalGrid (datatypes/inc/grid.h:2038-2158) stores only a window of the
+ * domain: select_region origin o and dims d in storage coordinates, each
+ * including a BD-deep rim (grid.h:1222-1261), with its d0*d1*d2 values
+ * x-fastest; a position outside the window's interior reads `empty`
+ * (grid.h:1264-1277).  The solver evaluates the window's interior only
+ * (get_iterable_domain, datatypes/inc/dataiterator.h:2454-2470) with the
+ * window's own strides (sol/inc/stencil.h:209-240).  Here the window is an
+ * spo_sys whose storage is that buffer, its halo being the rim: along an axis
+ * the window spans from origin 0 the rim takes periodic images
+ * (regional_update_boundary, datatypes/inc/boundaryupdatedata.h:1397-1431);
+ * along any other axis it keeps what the last move wrote there (empty).
+ *
+ * The window follows the field (update_regional_system,
+ * sol/inc/boundarysystem.h:438-471): at the first update the cutoff becomes
+ * min + eps and `empty` the minimum (grid::min_value, boundarysystem.h:372-376),
+ * and the window is resized around the values >= cutoff; afterwards, every
+ * resize_delta of time, it is re-centred (fixed size) or resized again.
+ * The searches and moves restate datatypes/inc/gridfunctions.h:
+ *   get_view                   :1962-1986  (re-centre, size kept)
+ *   get_view_resized           :1873-1913  (bounding box; the reference runs it
+ *                                            under an OpenMP lock, in no fixed
+ *                                            order: here the serial order)
+ *   get_view_resized_periodic  :1988-2163  (box grown from the first value
+ *                                            >= cutoff, wrapping periodically)
+ *   adjust_region              :2166-2176, resize_adjust_region :2194-2238
+ *   adjust_region_to_from      :1662-1683  (new buffer of `empty`, interior
+ *                                            copied modulo the domain)
+ *   adjust_origin_to_from      :1770-1852  (shift in place; whether a cell
+ *                                            becomes empty is decided by the
+ *                                            last axis alone, and other cells
+ *                                            take the buffer value at
+ *                                            index + offset, rim included.
+ *                                            Here a gather from the old buffer,
+ *                                            so the overlaps of the in-place
+ *                                            order are not reproduced; a source
+ *                                            outside the buffer reads empty)
+ */
+
+typedef struct {
+  int D;
+  int G[3];  /* storage dims of the domain, n + 2 BD */
+  int o[3];  /* window origin (storage coordinates, rim included) */
+  int d[3];  /* window dims, rim included */
+  const double* v;  /* window buffer, d0*d1*d2 x-fastest (null when empty) */
+  double cut;
+} spo_rview;
+
+static long spo_rv_stride(const spo_rview* r, int a) {
+  long s = 1;
+  for (int i = 0; i < a; ++i) s *= r->d[i];
+  return s;
+}
+
+static long spo_rv_interior(const spo_rview* r, long c[3]) {
+  long len = 1;
+  for (int a = 0; a < r->D; ++a) {
+    c[a] = r->d[a] - 2 * BD;
+    if (c[a] <= 0) len = 0;
+    len *= (c[a] > 0 ? c[a] : 0);
+  }
+  return r->v ? len : 0;
+}
+
+/* get_view: buffer entries 0 .. len(interior)-1 (rim cells among them) at
+ * positions (n / stride) % interior_dims */
+static void spo_view_fixed(const spo_rview* r, int origin[3]) {
+  long c[3], iv[3][2], st[3];
+  const long len = spo_rv_interior(r, c);
+  for (int a = 0; a < r->D; ++a) {
+    iv[a][0] = c[a];
+    iv[a][1] = 0;
+    st[a] = spo_rv_stride(r, a);
+  }
+  for (long n = 0; n < len; ++n)
+    if (r->v[n] >= r->cut)
+      for (int a = 0; a < r->D; ++a) {
+        const long p = (n / st[a]) % c[a];
+        if (p < iv[a][0]) iv[a][0] = p;
+        if (p > iv[a][1]) iv[a][1] = p;
+      }
+  for (int a = 0; a < r->D; ++a) {
+    const long dims = iv[a][1] - iv[a][0] + 1 + 2 * BD;
+    const long delta = r->d[a] - dims;
+    origin[a] = (int)(r->o[a] + (iv[a][0] - delta / 2));
+  }
+}
+
+/* get_view_resized: bounding box of the interior values >= cutoff, serial order */
+static void spo_view_resized(const spo_rview* r, int origin[3], int dims[3]) {
+  long c[3], iv[3][2], st[3];
+  const long len = spo_rv_interior(r, c);
+  for (int a = 0; a < r->D; ++a) {
+    iv[a][0] = r->d[a];
+    iv[a][1] = 0;
+    st[a] = spo_rv_stride(r, a);
+  }
+  for (long n = 0; n < len; ++n) {
+    long pos[3], rem = n, idx = 0;
+    for (int a = 0; a < r->D; ++a) {
+      pos[a] = rem % c[a] + BD;
+      rem /= c[a];
+      idx += pos[a] * st[a];
+    }
+    if (!(r->v[idx] >= r->cut)) continue;
+    int inside = 1;
+    for (int a = 0; a < r->D; ++a) inside &= (pos[a] >= iv[a][0] && pos[a] < iv[a][1]);
+    if (inside) continue;
+    for (int a = 0; a < r->D; ++a) {
+      if (pos[a] >= iv[a][0]) {
+        if (pos[a] > iv[a][1]) iv[a][1] = pos[a];
+      } else if (pos[a] < iv[a][0]) {
+        iv[a][0] = pos[a];
+      }
+    }
+  }
+  for (int a = 0; a < r->D; ++a) {
+    origin[a] = (int)(iv[a][0] - BD + r->o[a]);
+    const long w = iv[a][1] - iv[a][0] + 1 + 2 * BD;
+    dims[a] = (int)(w > 0 ? w : 0);
+  }
+}
+
+static int spo_rv_at(const spo_rview* r, const long pos[3], const long st[3]) {
+  long idx = 0;
+  for (int a = 0; a < r->D; ++a) idx += (pos[a] + BD) * st[a];
+  return r->v[idx] >= r->cut;
+}
+
+/* get_view_resized_periodic: the window is the whole domain; grow a box from
+ * the first interior value >= cutoff, one slice at a time on each side of each
+ * axis, wrapping, until a pass changes nothing */
+static void spo_view_periodic(const spo_rview* r, int origin[3], int dims_out[3]) {
+  const int D = r->D;
+  long c[3], st[3];
+  const long len = spo_rv_interior(r, c);
+  for (int a = 0; a < D; ++a) st[a] = spo_rv_stride(r, a);
+  long start = -1;
+  for (long n = 0; n < len && start < 0; ++n) {
+    long pos[3], rem = n;
+    for (int a = 0; a < D; ++a) {
+      pos[a] = rem % c[a];
+      rem /= c[a];
+    }
+    if (spo_rv_at(r, pos, st)) start = n;
+  }
+  if (start < 0) {
+    for (int a = 0; a < D; ++a) dims_out[a] = 0;
+    return;
+  }
+  long iv[3][2], iu[3][2];
+  {
+    long rem = start;
+    for (int a = 0; a < D; ++a) {
+      iu[a][0] = iu[a][1] = rem % c[a];
+      rem /= c[a];
+    }
+  }
+  int grown;
+  do {
+    for (int a = 0; a < D; ++a) {
+      iv[a][0] = iu[a][0];
+      iv[a][1] = iu[a][1];
+    }
+    for (int i = 0; i < D; ++i) {
+      int right = 1;
+      long pos[3];
+      for (int j = 0; j < D; ++j) {
+        pos[j] = (j == i) ? iu[j][1] + 1 : iu[j][0];
+        /* the reference wraps a negative entry with the extent of axis i */
+        pos[j] = (pos[j] >= c[j]) ? pos[j] - c[j] : (pos[j] < 0) ? c[i] + pos[j] : pos[j];
+      }
+      long sd[2] = {1, 1};
+      int ns = 0;
+      for (int j = 0; j < D; ++j)
+        if (j != i) sd[ns++] = iu[j][1] - iu[j][0] + 1;
+      long slen = 1;
+      for (int q = 0; q < ns; ++q) slen *= sd[q];
+      const long steps = c[i] - (iu[i][1] - iu[i][0] + 1);
+      int found[2] = {1, 0};
+      long last[2] = {iu[i][0], iu[i][1]};
+      for (long n = 0; n < steps; ++n) {
+        for (long m = 0; m < slen && !found[right ? 1 : 0]; ++m) {
+          long sp[2] = {m % sd[0], ns > 1 ? m / sd[0] : 0};
+          int q = 0;
+          for (int j = 0; j < D; ++j) {
+            if (j == i) continue;
+            long p = sp[q++] + iu[j][0];
+            pos[j] = (p < 0) ? p + c[j] : (p >= c[j]) ? p - c[j] : p;
+          }
+          if (spo_rv_at(r, pos, st)) found[right ? 1 : 0] = 1;
+        }
+        if (right) {
+          if (found[1]) {
+            iu[i][1] = (pos[i] < iu[i][1]) ? pos[i] + c[i] : pos[i];
+            ++last[1];
+          }
+          pos[i] = (last[0] <= 0) ? c[i] + last[0] - 1 : last[0] - 1;
+          found[0] = 0;
+          right = 0;
+        } else {
+          if (found[0]) {
+            iu[i][0] = (pos[i] > iu[i][0]) ? pos[i] - c[i] : pos[i];
+            --last[0];
+          }
+          pos[i] = (last[1] >= c[i] - 1) ? last[1] + 1 - c[i] : last[1] + 1;
+          found[1] = 0;
+          right = 1;
+        }
+      }
+    }
+    grown = 0;
+    for (int a = 0; a < D; ++a) grown |= !(iv[a][0] <= iu[a][0] && iv[a][1] >= iu[a][1]);
+  } while (grown);
+  for (int a = 0; a < D; ++a) {
+    origin[a] = (int)(iu[a][0] + r->o[a]);
+    const long w = iu[a][1] - iu[a][0] + 1 + 2 * BD;
+    dims_out[a] = (int)(w > 0 ? w : 0);
+  }
+}
+
+/* The window the next move goes to.  mode 0: adjust_region (re-centred, dims
+ * kept, origin wrapped into the domain); mode 1: resize_adjust_region with
+ * padding factor `factor` and relative-dims tolerance `rel_eps`. */
+static void spo_view_target(const spo_rview* r, int mode, double factor, double rel_eps,
+                            int no[3], int nd[3]) {
+  const int D = r->D;
+  for (int a = 0; a < 3; ++a) {
+    no[a] = r->o[a];
+    nd[a] = r->d[a];
+  }
+  if (mode == 0) {
+    int origin[3] = {0, 0, 0};
+    spo_view_fixed(r, origin);
+    for (int a = 0; a < D; ++a) {
+      const int delta = r->G[a] - 2 * BD;
+      no[a] = origin[a] + ((origin[a] < 0) ? delta : (origin[a] >= delta) ? -delta : 0);
+    }
+    return;
+  }
+  int origin[3] = {0, 0, 0}, dims[3] = {0, 0, 0};
+  int whole = 1;
+  for (int a = 0; a < D; ++a) whole &= (r->G[a] == r->d[a]);
+  if (whole)
+    spo_view_periodic(r, origin, dims);
+  else
+    spo_view_resized(r, origin, dims);
+  int same = 1;
+  for (int a = 0; a < D; ++a) {
+    int scaled = (int)(dims[a] * factor);
+    const int dim0 = r->G[a] < scaled ? r->G[a] : scaled;
+    no[a] = origin[a] - (dim0 - dims[a]) / 2;
+    no[a] += (no[a] < 0) ? (r->G[a] - 2 * BD) : 0;
+    nd[a] = dim0;
+    if (abs(nd[a] - r->d[a]) / (double)r->d[a] > rel_eps) same = 0;
+  }
+  if (same) {
+    for (int a = 0; a < D; ++a) {
+      no[a] = origin[a] - (r->d[a] - dims[a]) / 2;
+      no[a] += (no[a] < 0) ? (r->G[a] - 2 * BD) : 0;
+      nd[a] = r->d[a];
+    }
+  }
+}
+
+/* exported for the host-logic tests: the target window of a buffer of values */
+int spo_reg_search(int dim, const int G[3], const int o[3], const int d[3], const double* buf,
+                   double cutoff, int mode, double factor, double rel_eps, int no[3], int nd[3]) {
+  spo_rview r;
+  memset(&r, 0, sizeof(r));
+  r.D = dim;
+  for (int a = 0; a < 3; ++a) {
+    r.G[a] = a < dim ? G[a] : 1;
+    r.o[a] = a < dim ? o[a] : 0;
+    r.d[a] = a < dim ? d[a] : 1;
+  }
+  r.v = buf;
+  r.cut = cutoff;
+  spo_view_target(&r, mode, factor, rel_eps, no, nd);
+  return 0;
+}
+
+typedef struct {
+  spo_desc gd;  /* the whole system (n = domain interior) */
+  int D;
+  int G[3], o[3], d[3];
+  double empty, cutoff, time;
+  int next_resize;
+  double delta, factor, eps;
+  int fixed, threads, has;
+  spo_sys sys;  /* the window (valid when has) */
+} spo_reg;
+
+static long spo_mod(long a, long n) {
+  long r = a % n;
+  return r < 0 ? r + n : r;
+}
+
+static void spo_reg_build(spo_reg* r) {
+  spo_desc w = r->gd;
+  r->has = 1;
+  for (int a = 0; a < r->D; ++a) {
+    w.n[a] = r->d[a] - 2 * BD;
+    if (w.n[a] <= 0) r->has = 0;
+    const int whole = (r->o[a] == 0 && r->d[a] == r->G[a]);
+    w.bc[2 * a] = w.bc[2 * a + 1] = whole ? SPO_PERIODIC : SPO_DIRICHLET;
+    w.bcv[2 * a] = w.bcv[2 * a + 1] = r->empty;
+  }
+  if (!r->has) return;
+  spo_sys_init(&r->sys, &w, r->threads);
+  for (long i = 0; i < r->sys.g.size; ++i) r->sys.psi[0][i] = r->empty;
+}
+
+static void spo_reg_view(const spo_reg* r, spo_rview* v) {
+  memset(v, 0, sizeof(*v));
+  v->D = r->D;
+  for (int a = 0; a < 3; ++a) {
+    v->G[a] = r->G[a];
+    v->o[a] = r->o[a];
+    v->d[a] = r->d[a];
+  }
+  v->v = r->has ? r->sys.psi[0] : NULL;
+  v->cut = r->cutoff;
+}
+
+/* adjust_region_to_from / adjust_origin_to_from_replace: a new buffer of
+ * `empty`, interior cells copied from the old window modulo the domain */
+static void spo_reg_replace(spo_reg* r, const int no[3], const int nd[3]) {
+  spo_reg old = *r;
+  for (int a = 0; a < 3; ++a) {
+    r->o[a] = no[a];
+    r->d[a] = nd[a];
+  }
+  spo_reg_build(r);
+  if (r->has && old.has) {
+    long cn[3] = {1, 1, 1}, co[3] = {1, 1, 1}, delta[3] = {0, 0, 0};
+    for (int a = 0; a < r->D; ++a) {
+      const long wrap = r->G[a] - 2 * BD;
+      cn[a] = nd[a] - 2 * BD;
+      co[a] = old.d[a] - 2 * BD;
+      const long on = old.o[a] - wrap * lround((double)old.o[a] / wrap);
+      const long nn = no[a] - wrap * lround((double)no[a] / wrap);
+      delta[a] = nn - on;
+    }
+    const long len = cn[0] * cn[1] * cn[2];
+    for (long n = 0; n < len; ++n) {
+      long p[3] = {n % cn[0], (n / cn[0]) % cn[1], n / (cn[0] * cn[1])};
+      long q[3];
+      int in = 1;
+      for (int a = 0; a < 3; ++a) {
+        if (a < r->D) {
+          const long wrap = r->G[a] - 2 * BD;
+          q[a] = p[a] + delta[a];
+          q[a] = (q[a] < 0) ? q[a] + wrap : (q[a] >= wrap) ? q[a] - wrap : q[a];
+          in &= (q[a] >= 0 && q[a] < co[a]);
+        } else {
+          q[a] = 0;
+        }
+      }
+      if (!in) continue;
+      const long dz = (r->D == 3) ? BD : 0;
+      const long ni = (p[0] + BD) + (p[1] + BD) * r->sys.g.s[1] + (p[2] + dz) * r->sys.g.s[2];
+      const long oi = (q[0] + BD) + (q[1] + BD) * old.sys.g.s[1] + (q[2] + dz) * old.sys.g.s[2];
+      r->sys.psi[0][ni] = old.sys.psi[0][oi];
+    }
+  }
+  if (old.has) spo_sys_free(&old.sys);
+}
+
+/* adjust_origin_to_from: the window keeps its dims */
+static void spo_reg_shift(spo_reg* r, const int no[3]) {
+  int skip = 1, replace = 0, dir[3] = {1, 1, 1};
+  for (int a = 0; a < r->D; ++a) {
+    const int delta = no[a] - r->o[a];
+    dir[a] = delta >= 0 ? 1 : -1;
+    skip &= (delta == 0);
+  }
+  if (skip) return;
+  for (int a = 0; a < r->D; ++a) replace |= (abs(no[a] - r->o[a]) + r->d[a] > r->G[a]);
+  if (replace || !r->has) {
+    spo_reg_replace(r, no, r->d);
+    return;
+  }
+  const long size = r->sys.g.size;
+  double* old = (double*)malloc(sizeof(double) * size);
+  memcpy(old, r->sys.psi[0], sizeof(double) * size);
+  long c[3] = {1, 1, 1}, ov[3] = {0, 0, 0}, off = 0, bo = 0;
+  for (int a = 0; a < r->D; ++a) {
+    c[a] = r->d[a] - 2 * BD;
+    const long sh = no[a] - r->o[a];
+    ov[a] = c[a] - (sh < 0 ? -sh : sh);
+    off += sh * r->sys.g.s[a];
+    bo += BD * r->sys.g.s[a];
+  }
+  const int L = r->D - 1;
+  const long len = c[0] * c[1] * c[2];
+  for (long n = 0; n < len; ++n) {
+    long p[3] = {n % c[0], (n / c[0]) % c[1], n / (c[0] * c[1])};
+    long idx = 0;
+    for (int a = 0; a < r->D; ++a) idx += p[a] * r->sys.g.s[a];
+    const int set_empty = dir[L] > 0 ? (p[L] >= ov[L]) : (p[L] < c[L] - ov[L]);
+    const long src = idx + off + bo;
+    r->sys.psi[0][idx + bo] =
+        (set_empty || src < 0 || src >= size) ? r->empty : old[src];
+  }
+  free(old);
+  for (int a = 0; a < 3; ++a) r->o[a] = no[a];
+}
+
+/* RegionalGrid::adjust(select_region) (grid.h:2118-2128) */
+static void spo_reg_move(spo_reg* r, const int no[3], const int nd[3]) {
+  int same_d = 1, same_o = 1;
+  for (int a = 0; a < r->D; ++a) {
+    same_d &= (nd[a] == r->d[a]);
+    same_o &= (no[a] == r->o[a]);
+  }
+  if (same_d && same_o) return;
+  if (same_d)
+    spo_reg_shift(r, no);
+  else
+    spo_reg_replace(r, no, nd);
+}
+
+/* grid::min_value of a RegionalGrid: the whole buffer, then empty */
+static double spo_reg_min(const spo_reg* r) {
+  double m = r->empty;
+  if (r->has) {
+    double e = r->sys.psi[0][0];
+    for (long i = 1; i < r->sys.g.size; ++i)
+      if (r->sys.psi[0][i] < e) e = r->sys.psi[0][i];
+    m = (r->empty < e) ? r->empty : e;
+  }
+  return m;
+}
+
+static void spo_reg_update(spo_reg* r) {
+  spo_rview v;
+  int no[3], nd[3];
+  if (r->next_resize == 0) {
+    const double m0 = spo_reg_min(r);
+    r->cutoff = m0 + r->eps;
+    r->empty = m0;
+    if (r->has)
+      for (int s = 0; s < 6; ++s) r->sys.d.bcv[s] = r->empty;
+    spo_reg_view(r, &v);
+    spo_view_target(&v, 1, r->factor, 0.0, no, nd);
+    spo_reg_move(r, no, nd);
+    ++r->next_resize;
+  } else if (r->next_resize > 0) {
+    const int cur = (int)(r->time / r->delta);
+    if (cur >= r->next_resize) {
+      spo_reg_view(r, &v);
+      spo_view_target(&v, r->fixed ? 0 : 1, r->factor, 0.05, no, nd);
+      spo_reg_move(r, no, nd);
+      r->next_resize = cur + 1;
+    }
+  }
+}
+
+void* spo_reg_create(const spo_desc* d, double resize_delta, double factor, double eps, int fixed,
+                     int threads) {
+  spo_reg* r = (spo_reg*)calloc(1, sizeof(spo_reg));
+  r->gd = *d;
+  r->D = d->dim;
+  for (int a = 0; a < 3; ++a) {
+    r->G[a] = a < d->dim ? d->n[a] + 2 * BD : 1;
+    r->o[a] = 0;
+    r->d[a] = r->G[a];
+  }
+  r->empty = 0.0; /* REGIONAL_GRID_OUTER_VALUE, datatypes/inc/grid.h:2022 */
+  r->delta = resize_delta;
+  r->factor = factor;
+  r->eps = eps;
+  r->fixed = fixed;
+  r->threads = threads > 0 ? threads : 1;
+  spo_reg_build(r);
+  return r;
+}
+
+/* whole-domain interior values in (x-fastest); the window takes its cells */
+void spo_reg_set(void* h, const double* global) {
+  spo_reg* r = (spo_reg*)h;
+  if (!r->has) return;
+  const long c0 = r->d[0] - 2 * BD, c1 = r->d[1] - 2 * BD, c2 = r->D == 3 ? r->d[2] - 2 * BD : 1;
+  const long n0 = r->gd.n[0], n1 = r->gd.n[1], n2 = r->D == 3 ? r->gd.n[2] : 1;
+  const long dz = (r->D == 3) ? BD : 0;
+  for (long k = 0; k < c2; ++k)
+    for (long j = 0; j < c1; ++j)
+      for (long i = 0; i < c0; ++i) {
+        const long gx = spo_mod(r->o[0] + i, n0), gy = spo_mod(r->o[1] + j, n1);
+        const long gz = r->D == 3 ? spo_mod(r->o[2] + k, n2) : 0;
+        r->sys.psi[0][(i + BD) + (j + BD) * r->sys.g.s[1] + (k + dz) * r->sys.g.s[2]] =
+            global[gx + n0 * (gy + n1 * gz)];
+      }
+  spo_update_halo(&r->sys.d, &r->sys.g, r->sys.psi[0]);
+}
+
+/* whole-domain interior values out: empty outside the window's interior */
+void spo_reg_get(void* h, double* global) {
+  spo_reg* r = (spo_reg*)h;
+  const long n0 = r->gd.n[0], n1 = r->gd.n[1], n2 = r->D == 3 ? r->gd.n[2] : 1;
+  for (long i = 0; i < n0 * n1 * n2; ++i) global[i] = r->empty;
+  if (!r->has) return;
+  const long c0 = r->d[0] - 2 * BD, c1 = r->d[1] - 2 * BD, c2 = r->D == 3 ? r->d[2] - 2 * BD : 1;
+  const long dz = (r->D == 3) ? BD : 0;
+  for (long k = 0; k < c2; ++k)
+    for (long j = 0; j < c1; ++j)
+      for (long i = 0; i < c0; ++i) {
+        const long gx = spo_mod(r->o[0] + i, n0), gy = spo_mod(r->o[1] + j, n1);
+        const long gz = r->D == 3 ? spo_mod(r->o[2] + k, n2) : 0;
+        global[gx + n0 * (gy + n1 * gz)] =
+            r->sys.psi[0][(i + BD) + (j + BD) * r->sys.g.s[1] + (k + dz) * r->sys.g.s[2]];
+      }
+}
+
+/* n iterations of run_model: update(time), equation, step, time += dt */
+void spo_reg_step(void* h, int nsteps) {
+  spo_reg* r = (spo_reg*)h;
+  for (int i = 0; i < nsteps; ++i) {
+    spo_reg_update(r);
+    if (r->has) spo_sys_step(&r->sys);
+    r->time += r->gd.dt;
+  }
+}
+
+void spo_reg_adjust(void* h, const int o[3], const int d[3]) {
+  spo_reg* r = (spo_reg*)h;
+  int no[3] = {0, 0, 0}, nd[3] = {1, 1, 1};
+  for (int a = 0; a < r->D; ++a) {
+    no[a] = o[a];
+    nd[a] = d[a];
+  }
+  spo_reg_move(r, no, nd);
+}
+
+/* window origin and dims; state = {empty, cutoff, time, next_resize} */
+void spo_reg_window(void* h, int o[3], int d[3], double state[4]) {
+  spo_reg* r = (spo_reg*)h;
+  for (int a = 0; a < 3; ++a) {
+    o[a] = r->o[a];
+    d[a] = r->d[a];
+  }
+  state[0] = r->empty;
+  state[1] = r->cutoff;
+  state[2] = r->time;
+  state[3] = r->next_resize;
+}
+
+void spo_reg_destroy(void* h) {
+  spo_reg* r = (spo_reg*)h;
+  if (r->has) spo_sys_free(&r->sys);
+  free(r);
+}

@@ -55,6 +55,18 @@ def _load():
     lib.spo_get.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
     lib.spo_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.spo_destroy.argtypes = [ctypes.c_void_p]
+    ip = ctypes.POINTER(ctypes.c_int)
+    lib.spo_reg_create.argtypes = [ctypes.POINTER(Desc), ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    lib.spo_reg_create.restype = ctypes.c_void_p
+    lib.spo_reg_set.argtypes = [ctypes.c_void_p, dp]
+    lib.spo_reg_get.argtypes = [ctypes.c_void_p, dp]
+    lib.spo_reg_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.spo_reg_adjust.argtypes = [ctypes.c_void_p, ip, ip]
+    lib.spo_reg_window.argtypes = [ctypes.c_void_p, ip, ip, dp]
+    lib.spo_reg_destroy.argtypes = [ctypes.c_void_p]
+    lib.spo_reg_search.argtypes = [ctypes.c_int, ip, ip, ip, dp, ctypes.c_double, ctypes.c_int,
+                                   ctypes.c_double, ctypes.c_double, ip, ip]
     return lib
 
 
@@ -157,3 +169,62 @@ class System:
 
     def __del__(self):
         self.close()
+
+
+def _i3(v):
+    a = (ctypes.c_int * 3)(0, 0, 0)
+    for i, x in enumerate(v):
+        a[i] = int(x)
+    return a
+
+
+class Regional:
+    """The oracle's regional system (the moving window of SolverSystemFDwSD):
+    whole-domain fields in and out, `empty` outside the window's interior."""
+
+    def __init__(self, d, field, resize_delta=3.0, factor=2.0, eps=1e-6, fixed=True, threads=1):
+        self.d = d
+        self.h = _lib.spo_reg_create(ctypes.byref(d), float(resize_delta), float(factor),
+                                     float(eps), int(bool(fixed)), int(threads))
+        self.set(field)
+
+    def set(self, field):
+        a = np.ascontiguousarray(field, dtype=np.float64).reshape(shape_of(self.d))
+        _lib.spo_reg_set(self.h, _ptr(a))
+
+    def get(self):
+        out = np.empty(shape_of(self.d), dtype=np.float64)
+        _lib.spo_reg_get(self.h, _ptr(out))
+        return out
+
+    def step(self, n=1):
+        _lib.spo_reg_step(self.h, int(n))
+
+    def adjust(self, origin, dims):
+        _lib.spo_reg_adjust(self.h, _i3(origin), _i3(dims))
+
+    def window(self):
+        """(origin, dims, empty, cutoff, time, next_resize) of the window."""
+        o, dd = _i3(()), _i3(())
+        st = (ctypes.c_double * 4)()
+        _lib.spo_reg_window(self.h, o, dd, st)
+        D = self.d.dim
+        return (tuple(o[:D]), tuple(dd[:D]), st[0], st[1], st[2], int(st[3]))
+
+    def close(self):
+        if self.h:
+            _lib.spo_reg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def reg_search(dim, G, o, d, buf, cutoff, mode, factor=2.0, rel_eps=0.0):
+    """Target window (origin, dims) of the oracle's search on a window buffer
+    of values (rim included, x-fastest): mode 0 re-centres, mode 1 resizes."""
+    b = np.ascontiguousarray(buf, dtype=np.float64).ravel()
+    no, nd = _i3(()), _i3(())
+    _lib.spo_reg_search(int(dim), _i3(G), _i3(o), _i3(d), _ptr(b), float(cutoff), int(mode),
+                        float(factor), float(rel_eps), no, nd)
+    return tuple(no[:dim]), tuple(nd[:dim])

@@ -67,6 +67,15 @@ class SpMember(ctypes.Structure):
     ]
 
 
+class SpRegionalParams(ctypes.Structure):
+    _fields_ = [
+        ("resize_delta", ctypes.c_double),
+        ("padding_factor", ctypes.c_double),
+        ("cutoff_eps", ctypes.c_double),
+        ("fixed", ctypes.c_int),
+    ]
+
+
 _H = ctypes.c_void_p
 _P = ctypes.c_void_p
 _SZ = ctypes.c_size_t
@@ -117,6 +126,24 @@ SIGNATURES = {
                                     ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int,
                                     ctypes.c_float, _P]),
     "sp_conserve_mass": (ctypes.c_int, [_H, ctypes.c_int]),
+    "sp_regional_create": (ctypes.c_int, [ctypes.POINTER(SpDesc), ctypes.POINTER(SpRegionalParams),
+                                          ctypes.POINTER(_P)]),
+    "sp_regional_upload": (ctypes.c_int, [_P, _P, _SZ]),
+    "sp_regional_download": (ctypes.c_int, [_P, _P, _SZ]),
+    "sp_regional_step": (ctypes.c_int, [_P, ctypes.c_int]),
+    "sp_regional_adjust": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int)]),
+    "sp_regional_window": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_double)]),
+    "sp_regional_handle": (_H, [_P]),
+    "sp_regional_error": (ctypes.c_char_p, [_P]),
+    "sp_regional_destroy": (None, [_P]),
+    "sp_region_search": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                        _P, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                        ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int)]),
     "sp_noalloc_error": (ctypes.c_char_p, []),
     "sp_last_error": (ctypes.c_char_p, [_H]),
     "sp_create_error": (ctypes.c_char_p, []),
