@@ -1,7 +1,7 @@
 """Throughput of the fused forward-Euler finite-difference step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload b3d|ensemble|c3d]
+                    [--workload b3d|ensemble|c3d|regional]
 
 Workloads (synthetic seeded fields; site-updates/s counts interior sites
 advanced by one step, summed over instances):
@@ -21,6 +21,12 @@ advanced by one step, summed over instances):
   c3d       model C (psi conserved, eta not, gamma 0.5), 8 instances of 256^3
             periodic, dx 1, dt 0.005, FP32 fused, psi_bar 0.1 +- 0.1 and eta
             +-0.1; one launch advances all 8 (2.1 GB per buffer, beyond L2).
+  regional  model B 2D on a regional system (SymPhas's SolverSystemFDwSD):
+            one droplet of radius 200 in a 4096^2 periodic domain, FP32 fused,
+            dt 0.01; the window (about 1/15 of the domain) is re-centred every
+            3.0 of time.  Rates count the window's interior sites; the L2 is
+            flushed before every timed step; transfers of the end-to-end
+            number are whole-domain fields.
 
 With N > 1 (torchrun), every rank advances its own replica (the path runs on
 one GPU; replicas only) and the job time is the maximum over ranks.  Prints
@@ -55,7 +61,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="b3d", choices=["b3d", "ensemble", "c3d"])
+    ap.add_argument("--workload", default="b3d", choices=["b3d", "ensemble", "c3d", "regional"])
     ap.add_argument("--e2e-inner", type=int, default=100,
                     help="FD steps per end-to-end call (upload, steps, download)")
     return ap.parse_args()
@@ -283,7 +289,77 @@ class Ens:
             "(C restatement, %d threads over members)" % threads)
 
 
-WORKLOADS = {"b3d": B3D, "c3d": C3D, "ensemble": Ens}
+def droplet(n, radius, seed):
+    """FP64 field of a 2D n x n periodic domain: +1 (+-1e-3 seeded noise) inside
+    a disc of `radius` at the centre, -1 outside."""
+    import numpy as np
+
+    y, x = np.mgrid[0:n, 0:n]
+    inside = (x - n // 2) ** 2 + (y - n // 2) ** 2 < radius * radius
+    noise = np.random.default_rng(seed).uniform(-1e-3, 1e-3, (n, n))
+    return np.where(inside, 1.0 + noise, -1.0)
+
+
+class Reg2D:
+    """Model B 2D on a regional system: one droplet in a 4096^2 domain, FP32."""
+
+    name = "regional"
+    n = 4096
+    radius = 200
+    dt = 0.01
+    seed = 20261203
+    dtype = "f32"
+    bytes_per_site = 8
+    flush_each_step = True
+    kernel = "k_fd2d over the window's interior (the fused model B step of the window's handle)"
+    traffic_file = os.path.join(ROOT, "profiles", "k_fd2d_regional_window_f32.json")
+    workload = ("Cahn-Hilliard (model B) 2D regional system (SolverSystemFDwSD): one droplet of "
+                "radius 200 (+1 in -1) in a 4096^2 periodic domain, dx 1, dt 0.01, "
+                "Stencil2d2h<5,6,13>, fused step; window re-centred every 3.0 of time, padding "
+                "factor 2, cutoff min + 1e-6; site-updates counted over the window's interior")
+
+    def __init__(self, sp, rank, stream):
+        n = self.n
+        self.model = sp.RegionalModel(sp.model_MB_t, 2, sp.SolverFT(sp.Stencil2d2h(5, 6, 13),
+                                                                     form="fused"),
+                                      sp.ProblemParameters((n, n), h=1.0), dtype="f32",
+                                      dt=self.dt, resize_delta=3.0, padding_factor=2.0,
+                                      cutoff_eps=1e-6, fixed=True)
+        self.model.set_stream(stream.cuda_stream)
+        self.model.set_field(droplet(n, self.radius, self.seed + rank))
+        self.model.step(1)  # the first window check shrinks the window
+        self.shape = tune(self.model, 20)
+        self.sites = float(self.model.interior_sites())
+        # the window the timed steps run on (no re-centre falls due before 3.0 of time)
+        self.window = self.model.window()
+        self.fields = [(0, 0, n * n)]  # whole-domain transfers through the public API
+
+    def step(self, k):
+        self.model.step(k)
+
+    def config(self):
+        o, d = self.window
+        return {"domain": [self.n] * 2, "window_origin": list(o), "window_dims": list(d),
+                "window_interior_sites": int(self.sites),
+                "domain_sites_per_window_site": self.n * self.n / self.sites,
+                "kernel_shape": self.shape}
+
+    @classmethod
+    def cpu_system(cls, threads):
+        spo = oracle()
+        n = cls.n
+        d = spo.make_desc(2, (n, n), spo.MODEL_B, 1.0, cls.dt)
+        r = spo.Regional(d, droplet(n, cls.radius, cls.seed), resize_delta=3.0, factor=2.0,
+                         eps=1e-6, fixed=True, threads=threads)
+        r.step(1)
+        o, dims = r.window()[:2]
+        sites = float((dims[0] - 6) * (dims[1] - 6))
+        return (lambda: r.step(1)), sites, r.close, (
+            "SolverFT steps of the regional model B window (%d x %d interior) FP64 "
+            "(C restatement, %d threads)" % (dims[0] - 6, dims[1] - 6, threads))
+
+
+WORKLOADS = {"b3d": B3D, "c3d": C3D, "ensemble": Ens, "regional": Reg2D}
 
 
 def max_over_ranks(ms, dist, device="cuda"):

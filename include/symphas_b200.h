@@ -317,6 +317,9 @@ int sp_regional_adjust(sp_regional* r, const int origin[3], const int dims[3]);
 /* Origin and dims of the window; state = {empty, cutoff, time, next update
  * index}. */
 int sp_regional_window(const sp_regional* r, int origin[3], int dims[3], double state[4]);
+/* Run the regional system's work on `stream` (a cudaStream_t): the present
+ * window's handle and every window handle made later. */
+int sp_regional_set_stream(sp_regional* r, void* stream);
 /* The window's handle (null while the window has no interior): for
  * sp_kernel_info, sp_launch_count, sp_set_stream and the like. */
 sp_handle* sp_regional_handle(sp_regional* r);

@@ -444,6 +444,7 @@ struct sp_regional {
   double empty = 0.0, cutoff = 0.0, time = 0.0;
   int next_resize = 0;
   sp_handle* w = nullptr;  // the window (null while it has no interior)
+  void* stream = nullptr;  // stream given to every window handle, or null
   size_t esz = 8;
   std::string err;
 };
@@ -529,6 +530,13 @@ int make_window(sp_regional* R, const int o[3], const int d[3], sp_handle** out)
   }
   if (int rc = sp_create(&wd, out))
     return rfail(R, rc, std::string("window handle: ") + sp_create_error());
+  if (R->stream)
+    if (int rc = sp_set_stream(*out, R->stream)) {
+      const std::string why = sp_last_error(*out);
+      sp_destroy(*out);
+      *out = nullptr;
+      return rfail(R, rc, "window stream: " + why);
+    }
   return SP_OK;
 }
 
@@ -857,6 +865,14 @@ int sp_regional_window(const sp_regional* R, int origin[3], int dims[3], double 
     state[2] = R->time;
     state[3] = R->next_resize;
   }
+  return SP_OK;
+}
+
+int sp_regional_set_stream(sp_regional* R, void* stream) {
+  if (!R) return SP_EINVAL;
+  if (R->w)
+    if (int rc = sp_set_stream(R->w, stream)) return rfail(R, rc, sp_last_error(R->w));
+  R->stream = stream;
   return SP_OK;
 }
 

@@ -109,6 +109,22 @@ class RegionalModel:
         self._check(C.lib().sp_regional_download(self._r, out.ctypes.data, out.nbytes))
         return out
 
+    def upload_from(self, field, host_ptr, nbytes, inst=0):
+        """Whole-domain values from host memory at `host_ptr` (the Model
+        signature; field and inst must be 0)."""
+        if field != 0 or inst != 0:
+            raise ValueError("a regional system holds one field of one instance")
+        self._check(C.lib().sp_regional_upload(self._r, ctypes.c_void_p(host_ptr), int(nbytes)))
+
+    def download_to(self, field, host_ptr, nbytes, inst=0):
+        if field != 0 or inst != 0:
+            raise ValueError("a regional system holds one field of one instance")
+        self._check(C.lib().sp_regional_download(self._r, ctypes.c_void_p(host_ptr), int(nbytes)))
+
+    def set_stream(self, stream_ptr):
+        """Run all further work on the CUDA stream `stream_ptr`."""
+        self._check(C.lib().sp_regional_set_stream(self._r, ctypes.c_void_p(stream_ptr)))
+
     # --- stepping and the window ---------------------------------------------
     def step(self, n=1):
         self._check(C.lib().sp_regional_step(self._r, int(n)))
@@ -145,6 +161,22 @@ class RegionalModel:
         info = (ctypes.c_int * 8)()
         C.check(C.lib().sp_kernel_info(h, info), h)
         return list(info)
+
+    def autotune(self, reps=20):
+        """Time the tile shapes on the present window's handle, keep the fastest."""
+        h = self.handle()
+        if h is None:
+            return None
+        C.check(C.lib().sp_autotune(h, int(reps)), h)
+        return self.kernel_info()
+
+    def interior_sites(self):
+        """Sites of the window's interior (the sites a step advances)."""
+        o, d = self.window()
+        s = 1
+        for x in d:
+            s *= max(0, x - 6)
+        return s
 
     def launch_count(self):
         h = self.handle()

@@ -3,6 +3,8 @@ the time per step.  Used for timing and for profiling single launches:
 
     python -m symphas_b200.run --model B --dim 3 --n 256 --dtype f32 --steps 8
     python -m symphas_b200.run --ensemble 128 --steps 8     (2D AMK/BMK members)
+    python -m symphas_b200.run --regional 200 --n 4096 --steps 8
+                        (model B 2D, one droplet of that radius, regional window)
 
 Steps are launched one at a time (no CUDA graph), so a profiler sees each
 fused-step launch separately.
@@ -31,11 +33,17 @@ def main(argv=None):
     ap.add_argument("--ensemble", type=int, default=0,
                     help="run an ensemble of this many 2D members (sides 64..1024, models AMK "
                          "and BMK, FP32 fused) instead of one model")
+    ap.add_argument("--regional", type=int, default=0,
+                    help="run model B 2D on a regional system holding one droplet of this "
+                         "radius (+1 in -1) at the centre of an n x n domain; the first step "
+                         "shrinks the window, the steps after it are timed")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the fastest tile shape first (its launches come before the steps)")
     a = ap.parse_args(argv)
     if a.ensemble:
         return run_ensemble(a)
+    if a.regional:
+        return run_regional(a)
     st = sp.Stencil2d2h(5, 6, 13) if a.dim == 2 else sp.Stencil3d2h(7, 10, 25)
     cls = MODELS[a.model]
     coeff = a.coeff or ([0.5] if a.model == "C" else [])
@@ -73,6 +81,30 @@ def run_ensemble(a):
                       "form": a.form, "steps": a.steps, "wall_ms_per_step": 1e3 * el / a.steps,
                       "launches": e.launch_count(), "kernel": info}))
     e.close()
+
+
+def run_regional(a):
+    import numpy as np
+
+    n = a.n
+    y, x = np.mgrid[0:n, 0:n]
+    inside = (x - n // 2) ** 2 + (y - n // 2) ** 2 < a.regional ** 2
+    field = np.where(inside, 1.0 + np.random.default_rng(1).uniform(-1e-3, 1e-3, (n, n)), -1.0)
+    g = sp.RegionalModel(sp.model_MB_t, 2, sp.SolverFT(sp.Stencil2d2h(5, 6, 13), form=a.form),
+                         sp.ProblemParameters((n, n), h=a.h), dtype=a.dtype, dt=a.dt)
+    g.set_field(field)
+    g.step(1)
+    info = g.autotune(5) if a.autotune else g.kernel_info()
+    t0 = time.perf_counter()
+    g.step(a.steps)
+    g.get_field()
+    el = time.perf_counter() - t0
+    o, d = g.window()
+    print(json.dumps({"regional": a.regional, "n": n, "window_origin": o, "window_dims": d,
+                      "dtype": a.dtype, "form": a.form, "steps": a.steps,
+                      "wall_ms_per_step": 1e3 * el / a.steps, "launches": g.launch_count(),
+                      "kernel": info}))
+    g.close()
 
 
 if __name__ == "__main__":
