@@ -832,12 +832,20 @@ __global__ void __launch_bounds__(TC::NT)
   // Batches never overlap, so a CTA that finds an item past the end holds no
   // valid item in its next batch.  With few items per CTA, batches and items
   // held ahead would unbalance the tail: those launches take one item at a
-  // time, when they need it.
+  // time, when they need it -- except a single instance (no item list), whose
+  // tiles all cost the same: its CTAs take a fixed round-robin share, so no
+  // queue round trip to L2 lies on the path of a launch of a few tiles per CTA.
   const bool many = p.nitems >= 64 * int(gridDim.x);
+  const bool fixed_share = !many && !p.items;
   constexpr int QB = 4;
-  int qcur = 0, qend = 0, qnext = 0;
+  int qcur = 0, qend = 0, qnext = 0, qown = int(blockIdx.x);
   if (tid == 0 && many) qnext = atomicAdd(&p.ctr[0], QB);
   auto fetch = [&]() -> int2 {
+    if (fixed_share) {
+      const int t = qown;
+      qown += int(gridDim.x);
+      return t < p.nitems ? make_int2(0, t) : make_int2(-1, 0);
+    }
     if (qcur == qend) {
       if (many) {
         qcur = qnext;
@@ -950,7 +958,7 @@ __global__ void __launch_bounds__(TC::NT)
     }
   }
   __syncthreads();
-  if (tid == 0) {
+  if (tid == 0 && !fixed_share) {
     // the last CTA to leave the queue re-arms it for the next launch
     __threadfence();
     if (atomicAdd(&p.ctr[1], 1) == int(gridDim.x) - 1) {
