@@ -156,3 +156,27 @@ def test_regional_rejects_what_it_does_not_cover():
         g.adjust((0, 0), (8, 20))  # interior of 2 cells along x
     with pytest.raises(sp.SymPhasError):
         g.adjust((0, 0), (50, 20))  # wider than the domain's storage
+
+
+@pytest.mark.parametrize("model,fixed", [("BMK", False), ("AMK", True), ("A", False)])
+def test_regional_3d_other_models_and_modes(model, fixed):
+    dims = (30, 26, 28)
+    f = blob_field(dims, [(10, 16, 9)], 5, seed=9)
+    coeff = (0.8, 1.2) if model in ("AMK", "BMK") else (1.0, 1.0)
+    g, r = pair(model, 3, dims, f, delta=0.03, fixed=fixed, coeff=coeff)
+    for _ in range(3):
+        g.step(5)
+        r.step(5)
+        check_same(g, r)
+
+
+def test_regional_two_droplets_resize_f64_fused():
+    # the fused form in FP64 against the oracle's printed scheme: within the
+    # fused form's tolerance, and the same windows (no value near the cutoff)
+    dims = (80, 72)
+    f = blob_field(dims, [(20, 20), (55, 48)], 7, seed=5)
+    g, r = pair("B", 2, dims, f, form="fused", fixed=False, eps=0.05)
+    for _ in range(3):
+        g.step(8)
+        r.step(8)
+        check_same(g, r, exact=False, tol=1e-10)
