@@ -317,6 +317,9 @@ int sp_regional_adjust(sp_regional* r, const int origin[3], const int dims[3]);
 /* Origin and dims of the window; state = {empty, cutoff, time, next update
  * index}. */
 int sp_regional_window(const sp_regional* r, int origin[3], int dims[3], double state[4]);
+/* Change the time step of further sp_regional_step calls (the present
+ * window's handle and every window handle made later). */
+int sp_regional_set_dt(sp_regional* r, double dt);
 /* Run the regional system's work on `stream` (a cudaStream_t): the present
  * window's handle and every window handle made later. */
 int sp_regional_set_stream(sp_regional* r, void* stream);

@@ -136,6 +136,7 @@ SIGNATURES = {
     "sp_regional_window": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_double)]),
+    "sp_regional_set_dt": (ctypes.c_int, [_P, ctypes.c_double]),
     "sp_regional_set_stream": (ctypes.c_int, [_P, _P]),
     "sp_regional_handle": (_H, [_P]),
     "sp_regional_error": (ctypes.c_char_p, [_P]),

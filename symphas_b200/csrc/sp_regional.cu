@@ -868,6 +868,14 @@ int sp_regional_window(const sp_regional* R, int origin[3], int dims[3], double 
   return SP_OK;
 }
 
+int sp_regional_set_dt(sp_regional* R, double dt) {
+  if (!R) return SP_EINVAL;
+  if (R->w)
+    if (int rc = sp_set_dt(R->w, dt)) return rfail(R, rc, sp_last_error(R->w));
+  R->gd.dt = dt;
+  return SP_OK;
+}
+
 int sp_regional_set_stream(sp_regional* R, void* stream) {
   if (!R) return SP_EINVAL;
   if (R->w)

@@ -10,6 +10,7 @@
  *       (sol/inc/model.h:100-128)                             model_t<MA, SolverFT<Stencil2d2h<5, 6, 13>>, 2>
  *   symphas::find_solution(m, dt, steps) (modules-io.h:747-753)  find_solution(m, dt, steps)
  *   m.get_field<0>(), m.get_index(), m.get_time()             same
+ *   SolverSystemFDwSD (sol/inc/solversystem.h:62-77)          regional_model_t<...>
  *
  * The expression is the C++ type of sp_expr.cuh (op<I>() = op(I), c<I>() =
  * c(I), lap / bilap / gradlap / power<N>, and stage<K>() for operands staged
@@ -20,7 +21,8 @@
  *
  *   nvcc -std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a \
  *        --expt-relaxed-constexpr -I include -I symphas_b200/csrc \
- *        my_model.cu symphas_b200/csrc/sp_api.cu symphas_b200/csrc/sp_noalloc.cu -lcuda
+ *        my_model.cu symphas_b200/csrc/sp_api.cu symphas_b200/csrc/sp_noalloc.cu \
+ *        symphas_b200/csrc/sp_regional.cu -lcuda
  *
  * With SolverFT<..., true> (exact) and -fmad=false, FP64 results are
  * bit-identical to SymPhas's CPU solver when the expression is written in the
@@ -199,6 +201,104 @@ class model_t {
   sp_handle* h_ = nullptr;
   size_t n_;
   double dt_ = 0.0, time_ = 0.0;
+  int index_ = 0;
+};
+
+// Parameters of a regional system, SymPhas's command-line defaults
+// (regional-resize-time, -factor, -eps, -fixed; sol/src/boundarysystem.cpp:24-27).
+struct RegionalParameters {
+  double resize_delta = 3.0;
+  double padding_factor = 2.0;
+  double cutoff_eps = 1e-6;
+  bool fixed = true;
+};
+
+// A single-field model whose system is regional (SolverSystemFDwSD,
+// sol/inc/solversystem.h:62-77): only a window of the domain is stored and
+// stepped, and it follows the field (sp_regional_* in symphas_b200.h).  The
+// domain must be periodic; fields in and out are whole-domain interiors.
+// Compile sp_regional.cu with the runtime sources to use it.
+template <class MF, class Solver, int D, class T = double>
+class regional_model_t {
+ public:
+  static_assert(sp::model_of<MF>::nf == 1, "a regional system holds a single-field model");
+  static constexpr int nfields = 1;
+
+  regional_model_t(const double* coeff, size_t ncoeff, const ProblemParameters<D>& p,
+                   const RegionalParameters& rp = RegionalParameters())
+      : n_(1) {
+    using Sp = typename Solver::stencil;
+    sp_desc d{};
+    d.dim = D;
+    for (int a = 0; a < 3; ++a) d.n[a] = a < D ? p.n[a] : 1;
+    d.dtype = sizeof(T) == 8 ? SP_F64 : SP_F32;
+    d.model = detail::registered_id<MF, Solver, D, T>();
+    d.form = Solver::exact ? SP_FORM_EXACT : SP_FORM_FUSED;
+    d.lap_pts = Sp::lp;
+    d.gradlap_pts = Sp::gp;
+    d.bilap_pts = Sp::bp;
+    d.accuracy = Sp::acc;
+    for (int s = 0; s < 6; ++s) {
+      d.boundary[s] = p.boundary[s];
+      d.boundary_value[s] = p.boundary_value[s];
+    }
+    d.h = p.h;
+    for (int i = 0; i < 8; ++i) d.coeff[i] = i < int(ncoeff) ? coeff[i] : 1.0;
+    d.ncoeff = int(ncoeff);
+    d.batch = 1;
+    for (int a = 0; a < D; ++a) n_ *= size_t(p.n[a]);
+    const sp_regional_params q{rp.resize_delta, rp.padding_factor, rp.cutoff_eps,
+                               rp.fixed ? 1 : 0};
+    if (sp_regional_create(&d, &q, &r_) != SP_OK)
+      throw std::runtime_error(std::string("symphas_b200: ") + sp_regional_error(nullptr));
+  }
+  regional_model_t(const regional_model_t&) = delete;
+  regional_model_t& operator=(const regional_model_t&) = delete;
+  ~regional_model_t() { sp_regional_destroy(r_); }
+
+  // whole-domain interior values, x fastest (`empty` outside the window)
+  void set_field(int field, const std::vector<T>& v) {
+    check(field == 0 ? sp_regional_upload(r_, v.data(), v.size() * sizeof(T)) : SP_EINVAL);
+  }
+  std::vector<T> get_field(int field = 0) const {
+    std::vector<T> v(n_);
+    check(field == 0 ? sp_regional_download(r_, v.data(), v.size() * sizeof(T)) : SP_EINVAL);
+    return v;
+  }
+  template <size_t I>
+  std::vector<T> get_field() const {
+    return get_field(int(I));
+  }
+
+  // update(time) -- the window check -- runs inside step, before each iteration
+  void update(double = 0) {}
+  void equation() {}
+  void step(double dt, int n = 1) {
+    if (dt != dt_) {
+      check(sp_regional_set_dt(r_, dt));
+      dt_ = dt;
+    }
+    check(sp_regional_step(r_, n));
+    index_ += n;
+  }
+  int get_index() const { return index_; }
+  double get_time() const {
+    double st[4];
+    sp_regional_window(r_, nullptr, nullptr, st);
+    return st[2];
+  }
+  // window origin and dims (storage coordinates, rim included)
+  void window(int origin[3], int dims[3]) const { sp_regional_window(r_, origin, dims, nullptr); }
+  sp_regional* handle() { return r_; }
+
+ private:
+  void check(int rc) const {
+    if (rc != SP_OK)
+      throw std::runtime_error(std::string("symphas_b200: ") + sp_regional_error(r_));
+  }
+  sp_regional* r_ = nullptr;
+  size_t n_;
+  double dt_ = 0.0;
   int index_ = 0;
 };
 

@@ -129,6 +129,11 @@ class RegionalModel:
     def step(self, n=1):
         self._check(C.lib().sp_regional_step(self._r, int(n)))
 
+    def set_dt(self, dt):
+        """Time step of further steps."""
+        self._check(C.lib().sp_regional_set_dt(self._r, float(dt)))
+        self.dt = float(dt)
+
     def adjust(self, origin, dims):
         self._check(C.lib().sp_regional_adjust(self._r, _i3(origin), _i3(dims)))
 

@@ -60,3 +60,24 @@ def test_user_model_with_fourth_order_stencils(tmp_path):
     ref = spo.run(spo.make_desc(2, (n, n), spo.MODEL_A, h, dt, stencil=(9, 14, 21), acc=4),
                   spo.seed_uniform(seed, lo, hi, n * n).reshape(n, n), steps)
     assert np.array_equal(got, ref)
+
+
+def test_user_model_on_a_regional_system(tmp_path):
+    """The user-written MA on regional_model_t (SolverSystemFDwSD): the same
+    windows and whole-domain field as the oracle's regional system, bit for
+    bit in FP64."""
+    n, h, dt, steps = 80, 1.0, 0.01, 40
+    out = tmp_path / "psi.bin"
+    r = subprocess.run([EXE, "mareg", str(out), str(n), str(h), str(dt), str(steps), "0", "0", "0"],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(out, dtype=np.float64).reshape(n, n)
+    y, x = np.mgrid[0:n, 0:n]
+    rad, cx, cy = n / 5.0, n // 3, n // 2
+    f0 = np.where((x - cx) ** 2 + (y - cy) ** 2 < rad * rad, 1.0, -1.0)
+    ref = spo.Regional(spo.make_desc(2, (n, n), spo.MODEL_A, h, dt), f0, resize_delta=0.05)
+    ref.step(steps)
+    o, d = ref.window()[:2]
+    assert "window %d %d %d %d" % (o[0], o[1], d[0], d[1]) in r.stdout
+    assert d[0] < n + 6  # the window is smaller than the domain
+    assert np.array_equal(got, ref.get())
