@@ -445,6 +445,13 @@ struct sp_regional {
   int next_resize = 0;
   sp_handle* w = nullptr;  // the window (null while it has no interior)
   void* stream = nullptr;  // stream given to every window handle, or null
+  // device scratch, grown on demand and kept: whole-domain staging, a compact
+  // window, the cutoff mask, the minimum's partials (every use waits for its
+  // work before returning, so each call may reuse them)
+  struct Scratch {
+    void* p = nullptr;
+    size_t cap = 0;
+  } dom, win, msk, red;
   size_t esz = 8;
   std::string err;
 };
@@ -462,6 +469,19 @@ int rfail(sp_regional* R, int code, const std::string& msg) {
     cudaError_t e_ = (call);                                                       \
     if (e_ != cudaSuccess) return rfail(R, SP_ECUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
   } while (0)
+
+template <class P>
+int grow(sp_regional* R, sp_regional::Scratch& s, size_t bytes, P** out) {
+  if (s.cap < bytes) {
+    if (s.p) cudaFree(s.p);  // waits for the work that used it
+    s.p = nullptr;
+    s.cap = 0;
+    SP_RCUDA(R, cudaMalloc(&s.p, bytes));
+    s.cap = bytes;
+  }
+  *out = static_cast<P*>(s.p);
+  return SP_OK;
+}
 
 int blocks_for(long long n) { return int(std::max(1LL, std::min<long long>(148LL * 8, (n + 255) / 256))); }
 
@@ -547,13 +567,12 @@ int min_t(sp_regional* R, double* out) {
   const RegView<T> v = view_of<T>(R);
   const int blocks = blocks_for(interior_cells(R, R->d));
   T* part = nullptr;
-  SP_RCUDA(R, cudaMalloc(&part, sizeof(T) * blocks));
+  if (int rc = grow(R, R->red, sizeof(T) * blocks, &part)) return rc;
   k_reg_min<T><<<blocks, 256, 0, R->w->stream>>>(v, part);
   std::vector<T> h(blocks);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), part, sizeof(T) * blocks, cudaMemcpyDeviceToHost, R->w->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(R->w->stream);
-  cudaFree(part);
   if (e != cudaSuccess) return rfail(R, SP_ECUDA, std::string("window minimum: ") + cudaGetErrorString(e));
   T m = h[0];
   for (T x : h) m = x < m ? x : m;
@@ -570,12 +589,11 @@ int mask_t(sp_regional* R, std::vector<unsigned char>& mask) {
   const long long len = (long long)v.d[0] * v.d[1] * v.d[2];
   mask.resize(size_t(len));
   unsigned char* m = nullptr;
-  SP_RCUDA(R, cudaMalloc(&m, size_t(len)));
+  if (int rc = grow(R, R->msk, size_t(len), &m)) return rc;
   k_reg_mask<T><<<blocks_for(len), 256, 0, R->w->stream>>>(v, T(R->cutoff), m, len);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(mask.data(), m, size_t(len), cudaMemcpyDeviceToHost, R->w->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(R->w->stream);
-  cudaFree(m);
   if (e != cudaSuccess) return rfail(R, SP_ECUDA, std::string("window mask: ") + cudaGetErrorString(e));
   return SP_OK;
 }
@@ -617,9 +635,10 @@ int replace_t(sp_regional* R, const int no[3], const int nd[3]) {
       ov.cur = reinterpret_cast<const T*>(field_origin(nw, nw->cur, 0, 0));
     }
     T* tmp = nullptr;
+    if (rc == SP_OK) rc = grow(R, R->win, sizeof(T) * size_t(cells), &tmp);
     if (rc == SP_OK) {
-      cudaError_t e = cudaMalloc(&tmp, sizeof(T) * size_t(cells));
-      if (e == cudaSuccess) {
+      cudaError_t e = cudaSuccess;
+      {
         k_reg_remap<T><<<blocks_for(cells), 256, 0, nw->stream>>>(gn, ov, delta[0], delta[1],
                                                                    delta[2], T(R->empty), tmp);
         e = cudaGetLastError();
@@ -627,7 +646,6 @@ int replace_t(sp_regional* R, const int no[3], const int nd[3]) {
       if (e != cudaSuccess) rc = rfail(R, SP_ECUDA, std::string("window remap: ") + cudaGetErrorString(e));
     }
     if (rc == SP_OK) rc = put_window(R, nw, tmp, cells);
-    cudaFree(tmp);
   }
   if (rc != SP_OK) {
     if (nw) sp_destroy(nw);
@@ -654,17 +672,13 @@ int shift_t(sp_regional* R, const int no[3]) {
   if (replace || !R->w) return replace_t<T>(R, no, R->d);
   const long long cells = interior_cells(R, R->d);
   T* tmp = nullptr;
-  SP_RCUDA(R, cudaMalloc(&tmp, sizeof(T) * size_t(cells)));
+  if (int rc = grow(R, R->win, sizeof(T) * size_t(cells), &tmp)) return rc;
   const RegView<T> v = view_of<T>(R);
   k_reg_shift<T><<<blocks_for(cells), 256, 0, R->w->stream>>>(v, s[0], s[1], s[2], T(R->empty), tmp);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(R->w->stream);
-  if (e != cudaSuccess) {
-    cudaFree(tmp);
-    return rfail(R, SP_ECUDA, std::string("window shift: ") + cudaGetErrorString(e));
-  }
+  if (e != cudaSuccess) return rfail(R, SP_ECUDA, std::string("window shift: ") + cudaGetErrorString(e));
   const int rc = put_window(R, R->w, tmp, cells);
-  cudaFree(tmp);
   if (rc == SP_OK) std::copy(no, no + 3, R->o);
   return rc;
 }
@@ -770,9 +784,9 @@ int sp_regional_upload(sp_regional* R, const void* host, size_t bytes) {
   void* g = nullptr;
   void* win = nullptr;
   const long long cells = interior_cells(R, R->d);
-  SP_RCUDA(R, cudaMalloc(&g, bytes));
-  cudaError_t e = cudaMalloc(&win, size_t(cells) * R->esz);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(g, host, bytes, cudaMemcpyHostToDevice, R->w->stream);
+  if (int rc = grow(R, R->dom, bytes, &g)) return rc;
+  if (int rc = grow(R, R->win, size_t(cells) * R->esz, &win)) return rc;
+  cudaError_t e = cudaMemcpyAsync(g, host, bytes, cudaMemcpyHostToDevice, R->w->stream);
   if (e == cudaSuccess) {
     const Geo gg = geo_of(R, R->o, R->d);
     if (R->esz == 4)
@@ -784,8 +798,6 @@ int sp_regional_upload(sp_regional* R, const void* host, size_t bytes) {
   const int rc = e == cudaSuccess
                      ? put_window(R, R->w, win, cells)
                      : rfail(R, SP_ECUDA, std::string("regional upload: ") + cudaGetErrorString(e));
-  cudaFree(g);
-  cudaFree(win);
   return rc;
 }
 
@@ -803,7 +815,7 @@ int sp_regional_download(sp_regional* R, void* host, size_t bytes) {
     return SP_OK;
   }
   void* g = nullptr;
-  SP_RCUDA(R, cudaMalloc(&g, bytes));
+  if (int rc = grow(R, R->dom, bytes, &g)) return rc;
   const Geo gg = geo_of(R, R->o, R->d);
   if (R->esz == 4)
     k_reg_scatter<float><<<blocks_for(n), 256, 0, R->w->stream>>>(gg, view_of<float>(R), float(R->empty), (float*)g);
@@ -812,7 +824,6 @@ int sp_regional_download(sp_regional* R, void* host, size_t bytes) {
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(host, g, bytes, cudaMemcpyDeviceToHost, R->w->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(R->w->stream);
-  cudaFree(g);
   if (e != cudaSuccess) return rfail(R, SP_ECUDA, std::string("regional download: ") + cudaGetErrorString(e));
   return SP_OK;
 }
@@ -893,6 +904,8 @@ const char* sp_regional_error(const sp_regional* R) {
 void sp_regional_destroy(sp_regional* R) {
   if (!R) return;
   if (R->w) sp_destroy(R->w);
+  for (sp_regional::Scratch* sc : {&R->dom, &R->win, &R->msk, &R->red})
+    if (sc->p) cudaFree(sc->p);
   delete R;
 }
 
