@@ -637,12 +637,9 @@ int replace_t(sp_regional* R, const int no[3], const int nd[3]) {
     T* tmp = nullptr;
     if (rc == SP_OK) rc = grow(R, R->win, sizeof(T) * size_t(cells), &tmp);
     if (rc == SP_OK) {
-      cudaError_t e = cudaSuccess;
-      {
-        k_reg_remap<T><<<blocks_for(cells), 256, 0, nw->stream>>>(gn, ov, delta[0], delta[1],
-                                                                   delta[2], T(R->empty), tmp);
-        e = cudaGetLastError();
-      }
+      k_reg_remap<T><<<blocks_for(cells), 256, 0, nw->stream>>>(gn, ov, delta[0], delta[1],
+                                                                 delta[2], T(R->empty), tmp);
+      const cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) rc = rfail(R, SP_ECUDA, std::string("window remap: ") + cudaGetErrorString(e));
     }
     if (rc == SP_OK) rc = put_window(R, nw, tmp, cells);
