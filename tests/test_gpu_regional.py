@@ -180,3 +180,30 @@ def test_regional_two_droplets_resize_f64_fused():
         g.step(8)
         r.step(8)
         check_same(g, r, exact=False, tol=1e-10)
+
+
+def test_regional_fourth_order_stencils():
+    # Stencil2d4h<> reaches 3 cells (bilap): exactly the window's rim
+    dims = (72, 64)
+    f = blob_field(dims, [(30, 28)], 8, seed=12)
+    st = sp.Stencil2d4h()
+    g = sp.RegionalModel(sp.model_MA_t, 2, sp.SolverFT(st, form="exact"),
+                         sp.ProblemParameters(dims, h=1.0), coeff=(1.0, 1.0), dtype="f64",
+                         dt=0.01, resize_delta=0.05)
+    g.set_field(f)
+    r = spo.Regional(spo.make_desc(2, dims, spo.MODEL_A, 1.0, 0.01, coeff=(1.0, 1.0),
+                                   stencil=st.points, acc=4), f, resize_delta=0.05)
+    for _ in range(3):
+        g.step(8)
+        r.step(8)
+        check_same(g, r)
+
+
+def test_regional_3d_f32_fused():
+    dims = (40, 36, 32)
+    f = blob_field(dims, [(20, 18, 16)], 7, seed=4)
+    g, r = pair("B", 3, dims, f, dtype="f32", form="fused", delta=0.05, eps=0.05, dt=0.005)
+    for _ in range(3):
+        g.step(10)
+        r.step(10)
+        check_same(g, r, exact=False, tol=2e-5)
