@@ -339,7 +339,9 @@ int setup_2d_t(sp_handle* H) {
   std::vector<int2> items;
   for (int i : order) {
     const int tiles = ip[i].ntx * ((H->geo[i].n[1] + ty - 1) / ty);
-    for (int t = 0; t < tiles; ++t) items.push_back(make_int2(i, t));
+    // the tile's coordinates packed as x | y << 16 (sp::Step2Params::items)
+    for (int t = 0; t < tiles; ++t)
+      items.push_back(make_int2(i, (t % ip[i].ntx) | ((t / ip[i].ntx) << 16)));
   }
   H->nitems = int(items.size());
   H->ntx = ip[0].ntx;

@@ -71,7 +71,8 @@ struct Step2Params {
   const CUtensorMap* maps;  // input tensor maps, [inst * nf + f]
   T* const* out;            // output padded origins, [inst * nf + f]
   const Inst2<T>* inst;     // [ninst]
-  const int2* items;        // [nitems] (instance, tile) or null: instance 0, tile = item
+  const int2* items;        // [nitems] (instance, tile x | tile y << 16), or null:
+                            // instance 0, linear tile index = item
   int nitems;
   int* ctr;  // [0] work-queue counter, [1] finished-CTA counter; both are
              // zero on entry and the last CTA to finish zeroes them again
@@ -860,9 +861,16 @@ __global__ void __launch_bounds__(TC::NT)
     if (t >= p.nitems) return make_int2(-1, 0);
     return p.items ? p.items[t] : make_int2(0, t);
   };
+  // tile coordinates of an item: packed by the host in an item list (no
+  // division per tile), a linear index otherwise
+  auto tile_xy = [&](int t, int ntx) -> int2 {
+    if (p.items) return make_int2(t & 0xffff, t >> 16);
+    return make_int2(t % ntx, t / ntx);
+  };
   auto issue = [&](int2 it, int slot) {
     const Inst2<T>& ip = p.inst[it.x];
-    const int x0 = (it.y % ip.ntx) * TX, y0 = (it.y / ip.ntx) * TY;
+    const int2 tc = tile_xy(it.y, ip.ntx);
+    const int x0 = tc.x * TX, y0 = tc.y * TY;
     tma::mbar_arrive_expect_tx(&bars[slot], TXB);
 #pragma unroll
     for (int f = 0; f < NF; ++f)
@@ -946,7 +954,8 @@ __global__ void __launch_bounds__(TC::NT)
     {
       const Inst2<T>& ip = p.inst[cur.x];
       const T* sb = sbuf + (it & 1) * (NS > 0 ? NS : 1) * K::SPL;
-      const int x0 = (cur.y % ip.ntx) * TX, y0 = (cur.y / ip.ntx) * TY;
+      const int2 tc = tile_xy(cur.y, ip.ntx);
+      const int x0 = tc.x * TX, y0 = tc.y * TY;
       if (ip.kind == 0)
         fd2_out<K, M0, T, LP, GP, BP>(p, m0, ip, cur.x, fbuf, sb, it % NQ, x0, y0, msum);
       else
