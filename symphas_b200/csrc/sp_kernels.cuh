@@ -826,6 +826,16 @@ __global__ void __launch_bounds__(TC::NT)
   int xsr[K::NX1], xsc[K::NX1];
   extra_cells<NE, NT, K::NX, TY, RS, SWC, XC, TXT>(tid, xsr, xsc);
 
+  // Programmatic dependent launch: the host may start this grid while the
+  // previous step's grid drains.  Every thread waits here, before any global
+  // access (the work-queue counter the previous grid re-arms, the fields it
+  // wrote and the buffer it was still reading), until that grid has completed
+  // and its writes are visible; then lets the next step's grid be launched.
+  // Every launch of this kernel is persistent (all its CTAs resident at
+  // once), so the next grid's CTAs only take the slots this grid frees.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+
   // When every CTA has many items (ensembles), they are taken from the queue
   // in batches of 4, one batch requested ahead (thread 0 only): the atomic's
   // result is needed a batch later, so its round trip to L2 stays off the path

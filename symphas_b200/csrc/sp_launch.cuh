@@ -158,8 +158,20 @@ struct Entry2 {
     if (attr != cudaSuccess) return attr;
     const M0 m0 = MF0{}();
     const M1 m1 = MF1{}();
-    kern<<<grid, K::NT, K::SMEM, s>>>(*static_cast<const Step2Params<T>*>(prm), m0, m1);
-    return cudaGetLastError();
+    // programmatic stream serialization: the grid may launch while the
+    // previous kernel on the stream drains (k_fd2d waits for it before any
+    // global access)
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(K::NT);
+    cfg.dynamicSmemBytes = K::SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, *static_cast<const Step2Params<T>*>(prm), m0, m1);
   }
   static int occupancy() {
     auto kern = k_fd2d<M0, M1, T, LP, GP, BP, TC, EXACT>;
