@@ -172,6 +172,7 @@ struct Ch3 {
 template <class M, class T, class TC>
 __global__ void __launch_bounds__(TC::NT)
     k_ch3d(const __grid_constant__ StepParams<T> p, const __grid_constant__ M m) {
+  pdl_enter();
   using K = Ch3<M, T, TC>;
   constexpr int TX = K::TX, TY = K::TY, SPT = K::SPT, PD = K::PD, W = K::W, TXT = K::TXT,
                 R = K::R, RS = K::RS, RSA = K::RSA, HXA = K::HXA, PW = K::PW, PH = K::PH,

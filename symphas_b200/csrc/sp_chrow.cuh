@@ -352,11 +352,13 @@ __device__ __forceinline__ void chrow_step(const StepParams<float>& p, const M& 
 template <class M, class KC>
 __global__ void __launch_bounds__(KC::NT)
     k_chrow(const __grid_constant__ StepParams<float> p, const __grid_constant__ M m) {
+  pdl_enter();
   chrow_step<M, KC>(p, m);
 }
 template <class M, class KC>
 __global__ void __launch_bounds__(KC::NT, KC::MINB)
     k_chrow_occ(const __grid_constant__ StepParams<float> p, const __grid_constant__ M m) {
+  pdl_enter();
   chrow_step<M, KC>(p, m);
 }
 

@@ -220,4 +220,15 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return s;
 }
 
+// Programmatic dependent launch: every step kernel is launched with
+// programmatic stream serialization, so its grid may start while the previous
+// grid in the stream drains.  Every thread calls this before its first global
+// access: it waits until the previous grid has completed and its writes are
+// visible, then lets the next grid be launched (whose CTAs only take the
+// slots this grid frees: they start after all of this grid's CTAs have).
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 }  // namespace sp

@@ -342,6 +342,7 @@ __device__ __forceinline__ void extra_cells(int tid, int (&xsr)[NX > 0 ? NX : 1]
 template <class M, class T, int LP, int GP, int BP, class TC, bool EXACT>
 __global__ void __launch_bounds__(TC::NT)
     k_fd3d(const __grid_constant__ StepParams<T> p, const __grid_constant__ M m) {
+  pdl_enter();
   using K = Fd3<M, T, LP, GP, BP, TC, EXACT>;
   constexpr int TX = K::TX, TY = K::TY, SPT = K::SPT, PD = K::PD, W = K::W, TXT = K::TXT,
                 NF = K::NF, NS = K::NS, R = K::R, RS = K::RS, RSA = K::RSA, HXA = K::HXA,
@@ -826,15 +827,9 @@ __global__ void __launch_bounds__(TC::NT)
   int xsr[K::NX1], xsc[K::NX1];
   extra_cells<NE, NT, K::NX, TY, RS, SWC, XC, TXT>(tid, xsr, xsc);
 
-  // Programmatic dependent launch: the host may start this grid while the
-  // previous step's grid drains.  Every thread waits here, before any global
-  // access (the work-queue counter the previous grid re-arms, the fields it
-  // wrote and the buffer it was still reading), until that grid has completed
-  // and its writes are visible; then lets the next step's grid be launched.
-  // Every launch of this kernel is persistent (all its CTAs resident at
-  // once), so the next grid's CTAs only take the slots this grid frees.
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  // before any global access: the work-queue counter the previous grid
+  // re-arms, the fields it wrote and the buffer it was still reading
+  pdl_enter();
 
   // When every CTA has many items (ensembles), they are taken from the queue
   // in batches of 4, one batch requested ahead (thread 0 only): the atomic's

@@ -3,6 +3,8 @@
  */
 #pragma once
 
+#include <utility>
+
 #include "sp_ch.cuh"
 #include "sp_chrow.cuh"
 #include "sp_row.cuh"
@@ -11,6 +13,25 @@
 #include "sp_registry.h"
 
 namespace sp {
+
+// Launches a step kernel with programmatic stream serialization: its grid may
+// start while the previous kernel in the stream drains.  Every step kernel
+// calls pdl_enter() before its first global access.
+template <class... KArgs, class... Args>
+cudaError_t launch_step_kernel(void (*kern)(KArgs...), dim3 grid, int nt, size_t smem,
+                               cudaStream_t s, Args&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(nt);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 template <class MF>
 using model_of = decltype(MF{}());
@@ -25,8 +46,8 @@ struct Entry3 {
         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
     if (attr != cudaSuccess) return attr;
     const M m = MF{}();
-    kern<<<grid, K::NT, K::SMEM, s>>>(*static_cast<const StepParams<T>*>(prm), m);
-    return cudaGetLastError();
+    return launch_step_kernel(kern, grid, K::NT, K::SMEM, s,
+                              *static_cast<const StepParams<T>*>(prm), m);
   }
   static int occupancy() {
     auto kern = k_fd3d<M, T, LP, GP, BP, TC, EXACT>;
@@ -53,8 +74,8 @@ struct EntryCh3 {
         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
     if (attr != cudaSuccess) return attr;
     const M m = MF{}();
-    kern<<<grid, K::NT, K::SMEM, s>>>(*static_cast<const StepParams<T>*>(prm), m);
-    return cudaGetLastError();
+    return launch_step_kernel(kern, grid, K::NT, K::SMEM, s,
+                              *static_cast<const StepParams<T>*>(prm), m);
   }
   static int occupancy() {
     auto kern = k_ch3d<M, T, TC>;
@@ -88,8 +109,8 @@ struct EntryChRow {
         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
     if (attr != cudaSuccess) return attr;
     const M m = MF{}();
-    kern<<<grid, K::NT, K::SMEM, s>>>(*static_cast<const StepParams<float>*>(prm), m);
-    return cudaGetLastError();
+    return launch_step_kernel(kern, grid, K::NT, K::SMEM, s,
+                              *static_cast<const StepParams<float>*>(prm), m);
   }
   static int occupancy() {
     auto kern = kernel();
@@ -126,8 +147,8 @@ struct EntryRow {
         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
     if (attr != cudaSuccess) return attr;
     const M m = MF{}();
-    kern<<<grid, K::NT, K::SMEM, s>>>(*static_cast<const StepParams<float>*>(prm), m);
-    return cudaGetLastError();
+    return launch_step_kernel(kern, grid, K::NT, K::SMEM, s,
+                              *static_cast<const StepParams<float>*>(prm), m);
   }
   static int occupancy() {
     auto kern = kernel();
@@ -158,20 +179,8 @@ struct Entry2 {
     if (attr != cudaSuccess) return attr;
     const M0 m0 = MF0{}();
     const M1 m1 = MF1{}();
-    // programmatic stream serialization: the grid may launch while the
-    // previous kernel on the stream drains (k_fd2d waits for it before any
-    // global access)
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = grid;
-    cfg.blockDim = dim3(K::NT);
-    cfg.dynamicSmemBytes = K::SMEM;
-    cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kern, *static_cast<const Step2Params<T>*>(prm), m0, m1);
+    return launch_step_kernel(kern, grid, K::NT, K::SMEM, s,
+                              *static_cast<const Step2Params<T>*>(prm), m0, m1);
   }
   static int occupancy() {
     auto kern = k_fd2d<M0, M1, T, LP, GP, BP, TC, EXACT>;

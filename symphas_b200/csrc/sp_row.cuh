@@ -374,11 +374,13 @@ __device__ __forceinline__ void row_step(const StepParams<float>& p, const M& m)
 template <class M, class KC>
 __global__ void __launch_bounds__(KC::NT)
     k_row(const __grid_constant__ StepParams<float> p, const __grid_constant__ M m) {
+  pdl_enter();
   row_step<M, KC>(p, m);
 }
 template <class M, class KC>
 __global__ void __launch_bounds__(KC::NT, KC::MINB)
     k_row_occ(const __grid_constant__ StepParams<float> p, const __grid_constant__ M m) {
+  pdl_enter();
   row_step<M, KC>(p, m);
 }
 
