@@ -1221,9 +1221,8 @@ static void spo_reg_update(spo_reg* r) {
   if (r->next_resize == 0) {
     const double m0 = spo_reg_min(r);
     r->cutoff = m0 + r->eps;
-    r->empty = m0;
-    if (r->has)
-      for (int s = 0; s < 6; ++s) r->sys.d.bcv[s] = r->empty;
+    r->empty = m0; /* windows made from now on fill with it; the present
+                      window's rim keeps what its last move wrote there */
     spo_reg_view(r, &v);
     spo_view_target(&v, 1, r->factor, 0.0, no, nd);
     spo_reg_move(r, no, nd);

@@ -769,6 +769,13 @@ int sp_regional_create(const sp_desc* desc, const sp_regional_params* params, sp
     delete R;
     return rc;
   }
+  if (R->w && R->w->nf != 1) {
+    g_reg_create_error = "single-field models only (each field of SymPhas's multi-field models "
+                         "has a window of its own)";
+    sp_destroy(R->w);
+    delete R;
+    return SP_EINVAL;
+  }
   *out = R;
   return SP_OK;
 }

@@ -207,3 +207,26 @@ def test_regional_3d_f32_fused():
         g.step(10)
         r.step(10)
         check_same(g, r, exact=False, tol=2e-5)
+
+
+def test_regional_hand_set_window_keeps_its_rim():
+    # a window set by hand before the first step, which the first check keeps:
+    # `empty` becomes the minimum (-1) there, but the window's rim keeps the 0
+    # its move wrote (SymPhas rewrites a rim only when the window moves)
+    dims = (64, 56)
+    f = blob_field(dims, [(30, 26)], 7, seed=6)
+    probe = spo.Regional(spo.make_desc(2, dims, spo.MODEL_A, 1.0, 0.01, coeff=(1.0, 1.0)), f,
+                         resize_delta=0.05)
+    probe.step(1)
+    o, d = probe.window()[:2]
+    g, r = pair("A", 2, dims, f)
+    g.adjust(o, d)
+    r.adjust(o, d)
+    g.step(1)
+    r.step(1)
+    assert g.window() == (o, d) and g.state()[0] == -1.0  # kept by the first check
+    check_same(g, r)
+    for _ in range(3):
+        g.step(6)
+        r.step(6)
+        check_same(g, r)
