@@ -19,7 +19,9 @@
 #define SP_WIDE2(MODEL, MF0, MF1)                                                   \
   SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2w1); \
   SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2w2); \
-  SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2w3);
+  SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2w3); \
+  SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2d);  \
+  SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2e);
 
 namespace sp {
 void register_wide_kernels() {

@@ -276,6 +276,9 @@ template <> struct Tiles<float> {
   using D2w3 = TileCfg<128, 16, 2, 3, 4>;
   using D2b = TileCfg<64, 32, 4, 3, 2>;
   using D2c = TileCfg<128, 32, 8, 2, 2>;
+  // fewer tiles in flight, less shared memory: more CTAs per SM
+  using D2d = TileCfg<128, 16, 4, 2, 2>;
+  using D2e = TileCfg<128, 16, 4, 1, 2>;
 };
 template <> struct Tiles<double> {
   using D3 = TileCfg<64, 16, 2, 3, 2>;
