@@ -138,3 +138,37 @@ def test_library_search_matches_oracle_on_random_windows(D):
             eps = float(rng.choice([0.0, 0.05]))
             assert spo.reg_search(D, G, o, d, buf, 0.5, mode, f, eps) == \
                 sp.region_search(D, G, o, d, mask, mode, f, eps)
+
+
+def test_regional_create_rejects_without_a_gpu():
+    # argument checks come before any device call: they run on any machine
+    import ctypes
+
+    from symphas_b200 import _capi as C
+
+    def desc(**kw):
+        d = C.SpDesc()
+        d.dim, d.dtype, d.model, d.form = 2, C.SP_F64, C.SP_MODEL_A, C.SP_FORM_EXACT
+        d.n[0], d.n[1], d.n[2] = 32, 32, 1
+        d.lap_pts, d.gradlap_pts, d.bilap_pts = 5, 6, 13
+        d.h, d.dt, d.batch, d.accuracy = 1.0, 0.01, 1, 2
+        for k, v in kw.items():
+            setattr(d, k, v)
+        return d
+
+    p = C.SpRegionalParams()
+    p.resize_delta, p.padding_factor, p.cutoff_eps, p.fixed = 3.0, 2.0, 1e-6, 1
+    out = ctypes.c_void_p()
+    L = C.lib()
+    cases = [desc(model=C.SP_MODEL_C), desc(batch=2), desc(dim=4)]
+    d_dir = desc()
+    d_dir.boundary[0] = C.SP_DIRICHLET
+    cases.append(d_dir)
+    for d in cases:
+        assert L.sp_regional_create(ctypes.byref(d), ctypes.byref(p), ctypes.byref(out)) == C.SP_EINVAL
+        assert L.sp_regional_error(None)
+        assert not out.value
+    bad = C.SpRegionalParams()
+    bad.resize_delta, bad.padding_factor, bad.cutoff_eps = 0.0, 2.0, 1e-6
+    assert L.sp_regional_create(ctypes.byref(desc()), ctypes.byref(bad), ctypes.byref(out)) == C.SP_EINVAL
+    assert b"resize_delta" in L.sp_regional_error(None)
