@@ -230,3 +230,21 @@ def test_regional_hand_set_window_keeps_its_rim():
         g.step(6)
         r.step(6)
         check_same(g, r)
+
+
+def test_regional_on_a_caller_stream_across_window_replacements():
+    # a resizing window makes new window handles; each takes the caller's
+    # stream, and the results stay those of the oracle
+    torch = pytest.importorskip("torch")
+    dims = (96, 80)
+    f = blob_field(dims, [(40, 36)], 9, seed=8)
+    g, r = pair("B", 2, dims, f, fixed=False)
+    s = torch.cuda.Stream()
+    g.set_stream(s.cuda_stream)
+    handles = set()
+    for _ in range(4):
+        g.step(9)
+        r.step(9)
+        handles.add(g.handle())
+        check_same(g, r)
+    assert len(handles) > 1  # the window was replaced at least once
