@@ -26,11 +26,13 @@
  *     (sol/inc/modelspecialized.h:377-385, sol/inc/model.h:932-936), and the
  *     step is psi + dt*dframe over the interior (examples/solvers/solverft.h:46-50)
  *
- * Parity status: the SymPhas CPU solver could not be built here (its headers
- * need CMake-generated configuration files and two source patches for GCC 13),
- * so this restatement is pinned by known-answer tests (analytic stencil
- * results, the manufactured-solution convergence example of SymPhas,
- * conservation) rather than by outputs of SymPhas itself: parity unpinned.
+ * Parity status: pinned to SymPhas itself.  oracle/ref.mk compiles
+ * SymPhas's own CPU SolverFT from its sources (oracle/_ref/libsymphas_ref.so,
+ * wrapped by oracle/symref.py), and tests/test_ref_pin.py runs both on the
+ * same seeded inputs: bit-identical for the configurations, every stencil
+ * point set, unit-coefficient models A and B and the Dirichlet mixes SymPhas
+ * treats alike; within 1e-12 (about 5e-16) where SymPhas's optimiser folds
+ * non-unit coefficients into the terms in another order.
  *
  * Build: oracle/Makefile (gcc -O3 -ffp-contract=off -fopenmp -shared).
  * Floating-point contraction is disabled so every product and sum rounds on

@@ -2,7 +2,8 @@
 a GPU: published SplitMix64 outputs, analytic derivatives of smooth periodic
 fields (second-order convergence of every stencil point set), an independent
 numpy restatement, conservation, the Dirichlet halo rule, and the committed
-golden trajectories."""
+golden trajectories, the oracle's own and SymPhas's (the SymPhas solver itself
+is compared case by case in test_ref_pin.py)."""
 import os
 
 import numpy as np
@@ -154,3 +155,20 @@ def test_oracle_reproduces_golden_fixtures():
         out = spo.run(d, g[name + "_init"], steps)
         assert np.array_equal(out, g[name + "_final"]), name
     assert np.array_equal(g["splitmix_seed0_u01"], spo.seed_uniform(0, 0.0, 1.0, 8))
+
+
+def test_oracle_equals_symphas_golden_trajectories():
+    """Trajectories of SymPhas's own CPU SolverFT (written by
+    tests/golden/make_golden.py through oracle/ref.mk's build of SymPhas):
+    the first configuration (model A 2D 64^2, dx 0.5, dt 0.01, 1000 steps),
+    model B 3D 16^3 x 100 steps, model B on SymPhas's default
+    Stencil3d2h<15,10,25>.  The oracle reproduces every one bit for bit."""
+    g = np.load(os.path.join(HERE, "golden", "symphas_golden.npz"))
+    cases = {
+        "config_model_a_2d_64": (2, (64, 64), spo.MODEL_A, 0.5, 0.01, 1000, None),
+        "model_b_3d_16": (3, (16, 16, 16), spo.MODEL_B, 1.0, 0.005, 100, None),
+        "model_b_3d_default_stencil": (3, (12, 10, 8), spo.MODEL_B, 1.0, 0.002, 50, (15, 10, 25)),
+    }
+    for name, (dim, dims, model, h, dt, steps, st) in cases.items():
+        d = spo.make_desc(dim, dims, model, h, dt, stencil=st)
+        assert np.array_equal(spo.run(d, g[name + "_init"], steps), g[name + "_final"]), name
