@@ -32,9 +32,17 @@ With N > 1 (torchrun), every rank advances its own replica (the path runs on
 one GPU; replicas only) and the job time is the maximum over ranks.  Prints
 one JSON line (rank 0).
 
---impl reference times the CPU implementation of the same path (the C
-restatement of SymPhas's SolverFT in oracle/, FP64 as SymPhas computes, all
-host threads) on the same workload: a bounded sample per timed step.
+--impl reference times SymPhas's own CPU SolverFT (built from SymPhas's sources
+into oracle/_ref/ by oracle/ref.mk; FP64, SymPhas's only scalar type) on the
+same workload: one model per host thread, as SymPhas runs a model on one core
+(b3d: the one 256^3 model; c3d: the 8 instances; ensemble: every 8th member
+over all host threads).  SymPhas has no solver for the regional workload's
+window search here, so --workload regional times the oracle's C restatement
+(kind "port").  Without the built library every workload falls back to the
+restatement.
+
+--dtype f64 (b3d only) times the FP64 step in SymPhas's exact term order
+(bit-identical to SymPhas's own solver), 16 algorithmic bytes per site.
 """
 import argparse
 import json
@@ -62,6 +70,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="b3d", choices=["b3d", "ensemble", "c3d", "regional"])
+    ap.add_argument("--dtype", default="f32", choices=["f32", "f64"],
+                    help="b3d only: FP32 fused step (default) or the FP64 exact step")
     ap.add_argument("--e2e-inner", type=int, default=100,
                     help="FD steps per end-to-end call (upload, steps, download)")
     return ap.parse_args()
@@ -145,6 +155,14 @@ def oracle():
     return spo
 
 
+def symphas():
+    """SymPhas's own CPU solver (oracle/_ref), or None where it is not built."""
+    oracle()
+    import symref
+
+    return symref if symref.loaded() is not None else None
+
+
 class B3D:
     """Model B 3D 256^3 FP32 (the headline)."""
 
@@ -152,18 +170,19 @@ class B3D:
     n = 256
     dt = 0.005
     dtype = "f32"
+    form = "fused"
     bytes_per_site = 8  # one FP32 read and one FP32 write of the field per step
     flush_each_step = True
     kernel = "fused model B step (k_chrow / k_fd3d / k_ch3d, the autotuned tile variant)"
     traffic_file = os.path.join(ROOT, "profiles", "k_chrow_modelB_256cube_f32.json")
     workload = ("Cahn-Hilliard (model B) 3D 256^3 periodic, dx 1, dt 0.005, "
-                "Stencil3d2h<7,10,25>, fused step, psi_bar -0.2 +- 0.1 seeded noise")
+                "Stencil3d2h<7,10,25>, psi_bar -0.2 +- 0.1 seeded noise")
 
     def __init__(self, sp, rank, stream):
         n = self.n
         self.sites = float(n) ** 3
-        self.model = sp.model_MB_t(3, sp.SolverFT(sp.Stencil3d2h(7, 10, 25), form="fused"),
-                                   sp.ProblemParameters((n, n, n), h=1.0), dtype="f32")
+        self.model = sp.model_MB_t(3, sp.SolverFT(sp.Stencil3d2h(7, 10, 25), form=self.form),
+                                   sp.ProblemParameters((n, n, n), h=1.0), dtype=self.dtype)
         self.model.set_stream(stream.cuda_stream)
         self.model.fill_uniform(0, 20261203 + rank, -0.3, -0.1)
         self.shape = tune(self.model, 20)
@@ -173,17 +192,44 @@ class B3D:
         self.model.step(self.dt, k)
 
     def config(self):
-        return {"grid": [self.n] * 3, "kernel_shape": self.shape}
+        return {"grid": [self.n] * 3, "form": self.form, "kernel_shape": self.shape}
+
+    @classmethod
+    def initial(cls):
+        spo = oracle()
+        n = cls.n
+        return spo.seed_uniform(20261203, -0.3, -0.1, n ** 3).reshape(n, n, n)
+
+    @classmethod
+    def desc(cls):
+        spo = oracle()
+        n = cls.n
+        return spo.make_desc(3, (n, n, n), spo.MODEL_B, 1.0, cls.dt)
 
     @classmethod
     def cpu_system(cls, threads):
         spo = oracle()
-        n = cls.n
-        d = spo.make_desc(3, (n, n, n), spo.MODEL_B, 1.0, cls.dt)
-        x = spo.seed_uniform(20261203, -0.3, -0.1, n ** 3).reshape(n, n, n)
-        sysm = spo.System(d, x, threads)
-        return (lambda: sysm.step(1)), float(n) ** 3, sysm.close, (
+        sysm = spo.System(cls.desc(), cls.initial(), threads)
+        return (lambda: sysm.step(1)), float(cls.n) ** 3, sysm.close, (
             "SolverFT steps of model B 256^3 FP64 (C restatement, %d threads)" % threads)
+
+    @classmethod
+    def ref_system(cls, ref, threads):
+        """SymPhas's own solver on the same field: one model, one core."""
+        sysm = ref.System(cls.desc(), cls.initial())
+        return (lambda: sysm.step(1)), float(cls.n) ** 3, sysm.close, 1, (
+            "SymPhas SolverFT steps of model B 256^3 FP64 (one model: SymPhas runs it on "
+            "one core)")
+
+
+class B3D64(B3D):
+    """The same model B 256^3 step in FP64, SymPhas's exact term order."""
+
+    dtype = "f64"
+    form = "exact"
+    bytes_per_site = 16  # one FP64 read and one FP64 write of the field per step
+    kernel = "exact-form FP64 model B step (k_fd3d, the autotuned tile variant)"
+    traffic_file = os.path.join(ROOT, "profiles", "k_fd3d_modelB_256cube_f64.json")
 
 
 class C3D(B3D):
@@ -196,7 +242,7 @@ class C3D(B3D):
     kernel = "fused model C step (k_row / k_fd3d, two fields, the autotuned tile variant)"
     traffic_file = os.path.join(ROOT, "profiles", "k_row_modelC_8x256cube_f32.json")
     workload = ("model C (gamma 0.5) 3D, 8 instances of 256^3 periodic, dx 1, dt 0.005, "
-                "Stencil3d2h<7,10,25>, fused step, psi 0.1 +- 0.1, eta +- 0.1 seeded noise")
+                "Stencil3d2h<7,10,25>, psi 0.1 +- 0.1, eta +- 0.1 seeded noise")
 
     def __init__(self, sp, rank, stream):
         n = self.n
@@ -212,21 +258,42 @@ class C3D(B3D):
         self.fields = [(i, f, n ** 3) for i in range(self.batch) for f in range(2)]
 
     def config(self):
-        return {"grid": [self.n] * 3, "instances": self.batch, "kernel_shape": self.shape}
+        return {"grid": [self.n] * 3, "instances": self.batch, "form": self.form,
+                "kernel_shape": self.shape}
 
     @classmethod
-    def cpu_system(cls, threads):
+    def instance(cls, i):
         spo = oracle()
         import numpy as np
 
         n = cls.n
         d = spo.make_desc(3, (n, n, n), spo.MODEL_C, 1.0, cls.dt, coeff=(0.5,))
-        x = np.stack([spo.seed_uniform(7000, 0.0, 0.2, n ** 3),
-                      spo.seed_uniform(7001, -0.1, 0.1, n ** 3)]).reshape(2, n, n, n)
+        x = np.stack([spo.seed_uniform(7000 + 2 * i, 0.0, 0.2, n ** 3),
+                      spo.seed_uniform(7001 + 2 * i, -0.1, 0.1, n ** 3)]).reshape(2, n, n, n)
+        return d, x
+
+    @classmethod
+    def cpu_system(cls, threads):
+        spo = oracle()
+        d, x = cls.instance(0)
         sysm = spo.System(d, x, threads)
-        return (lambda: sysm.step(1)), float(n) ** 3, sysm.close, (
+        return (lambda: sysm.step(1)), float(cls.n) ** 3, sysm.close, (
             "SolverFT steps of one model C 256^3 instance FP64 (C restatement, %d threads)"
             % threads)
+
+    @classmethod
+    def ref_system(cls, ref, threads):
+        """SymPhas's own solver on the 8 instances, one model per core."""
+        systems = [ref.System(*cls.instance(i)) for i in range(cls.batch)]
+        used = min(threads, cls.batch)
+
+        def close():
+            for s in systems:
+                s.close()
+
+        return (lambda: ref.step_many(systems, 1, used)), float(cls.n) ** 3 * cls.batch, close, \
+            used, ("SymPhas SolverFT steps of the 8 model C 256^3 instances FP64 (%d threads, "
+                   "one model per thread)" % used)
 
 
 class Ens:
@@ -242,7 +309,7 @@ class Ens:
     traffic_file = os.path.join(ROOT, "profiles", "k_fd2d_ensemble1024_f32.json")
     workload = ("ensemble of 1024 2D periodic members, sides from {64,96,128,256,384,512,768,"
                 "1024}, half model A (AMK) half model B (BMK), M and kappa U[0.5,2], dt 40% of "
-                "each stability limit, Stencil2d2h<5,6,13>, fused step, +-0.1 seeded noise")
+                "each stability limit, Stencil2d2h<5,6,13>, +-0.1 seeded noise")
 
     def __init__(self, sp, rank, stream):
         self.members = sp.ensemble_members(self.count, seed=self.seed)
@@ -262,14 +329,12 @@ class Ens:
     def config(self):
         sides = sorted({m["dims"][0] for m in self.members})
         return {"members": self.count, "sides": sides, "sites": int(self.sites),
-                "kernel_shape": self.shape}
+                "form": "fused", "kernel_shape": self.shape}
 
     @classmethod
-    def cpu_system(cls, threads):
-        """Every 8th member (128 of them, both models, all sizes), all threads
-        over members (one member per thread, as independent SymPhas models)."""
+    def sample(cls):
+        """Every 8th member (128 of them, both models, all sizes)."""
         spo = oracle()
-        import numpy as np
 
         import symphas_b200.model as spm  # the member generator only (host code)
 
@@ -277,9 +342,32 @@ class Ens:
         ids = {"AMK": spo.MODEL_AMK, "BMK": spo.MODEL_BMK}
         descs = [spo.make_desc(2, m["dims"], ids[m["model"]], 1.0, m["dt"], coeff=m["coeff"])
                  for m in members]
-        fields = [spo.seed_uniform(cls.seed + i, -0.1, 0.1, m["dims"][0] * m["dims"][1])
-                  for i, m in enumerate(members)]
+        fields = [spo.seed_uniform(cls.seed + 8 * i, -0.1, 0.1, m["dims"][0] * m["dims"][1])
+                  .reshape(m["dims"][1], m["dims"][0]) for i, m in enumerate(members)]
         sites = float(sum(m["dims"][0] * m["dims"][1] for m in members))
+        return descs, fields, sites
+
+    @classmethod
+    def ref_system(cls, ref, threads):
+        """SymPhas's own solver on the sample, one model per thread."""
+        descs, fields, sites = cls.sample()
+        systems = [ref.System(d, f) for d, f in zip(descs, fields)]
+
+        def close():
+            for s in systems:
+                s.close()
+
+        return (lambda: ref.step_many(systems, 1, threads)), sites, close, threads, (
+            "one SymPhas SolverFT step of 128 of the 1024 members (every 8th) FP64 "
+            "(%d threads over members)" % threads)
+
+    @classmethod
+    def cpu_system(cls, threads):
+        """The sample, all threads over members (one member per thread, as
+        independent SymPhas models)."""
+        spo = oracle()
+        descs, fields, sites = cls.sample()
+        fields = [f.reshape(-1).copy() for f in fields]
 
         def one():
             spo.run_batch(descs, fields, [1] * len(descs), threads)
@@ -315,7 +403,7 @@ class Reg2D:
     traffic_file = os.path.join(ROOT, "profiles", "k_fd2d_regional_window_f32.json")
     workload = ("Cahn-Hilliard (model B) 2D regional system (SolverSystemFDwSD): one droplet of "
                 "radius 200 (+1 in -1) in a 4096^2 periodic domain, dx 1, dt 0.01, "
-                "Stencil2d2h<5,6,13>, fused step; window re-centred every 3.0 of time, padding "
+                "Stencil2d2h<5,6,13>; window re-centred every 3.0 of time, padding "
                 "factor 2, cutoff min + 1e-6; site-updates counted over the window's interior")
 
     def __init__(self, sp, rank, stream):
@@ -362,6 +450,14 @@ class Reg2D:
 WORKLOADS = {"b3d": B3D, "c3d": C3D, "ensemble": Ens, "regional": Reg2D}
 
 
+def workload(args):
+    if args.dtype == "f64":
+        if args.workload != "b3d":
+            raise SystemExit("--dtype f64 is built for --workload b3d only")
+        return B3D64
+    return WORKLOADS[args.workload]
+
+
 def max_over_ranks(ms, dist, device="cuda"):
     """The job's time: the slowest rank's (every rank gets it).  `dist` is
     torch.distributed when the job has more than one rank, else None."""
@@ -399,9 +495,15 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    W = WORKLOADS[args.workload]
+    W = workload(args)
     threads = os.cpu_count() or 1
-    step, sites, close, what = W.cpu_system(threads)
+    ref = symphas() if hasattr(W, "ref_system") else None
+    if ref is not None:
+        step, sites, close, cores, what = W.ref_system(ref, threads)
+        kind = "reference"
+    else:
+        step, sites, close, what = W.cpu_system(threads)
+        cores, kind = threads, "port"
     for _ in range(args.warmup):
         step()
     t0 = time.perf_counter()
@@ -416,8 +518,8 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": W.workload.replace("fused step", "SolverFT step")},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+        "config": {"workload": W.workload},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -442,7 +544,7 @@ def run_ours(args):
 
     import symphas_b200 as sp
 
-    W = WORKLOADS[args.workload]
+    W = workload(args)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     w = W(sp, rank, stream)
@@ -492,13 +594,14 @@ def run_ours(args):
 
     # end to end through the public API: every field of the step's input from
     # pinned host memory, e2e_inner steps, every field back to pinned memory
-    esz = 4
+    esz = 8 if W.dtype == "f64" else 4
     offs, total = [], 0
     for inst, f, cnt in w.fields:
         offs.append(total)
         total += cnt
-    host_in = torch.empty(total, dtype=torch.float32, pin_memory=True)
-    host_out = torch.empty(total, dtype=torch.float32, pin_memory=True)
+    tdt = torch.float64 if W.dtype == "f64" else torch.float32
+    host_in = torch.empty(total, dtype=tdt, pin_memory=True)
+    host_out = torch.empty(total, dtype=tdt, pin_memory=True)
     nbytes = total * esz
 
     def download(buf):
@@ -558,10 +661,13 @@ def run_ours(args):
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind, "kernel": W.kernel,
                      "alg_bytes_per_launch": alg_bytes},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes,
-                "d2h_bytes_per_step": nbytes,
-                "step": "upload every field from pinned host, %d fused steps, download every "
-                        "field" % args.e2e_inner},
+        # one call uploads every field, advances e2e_inner steps, downloads every
+        # field: bytes per FD step are the call's bytes over its steps
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes / args.e2e_inner,
+                "d2h_bytes_per_step": nbytes / args.e2e_inner, "steps_per_call": args.e2e_inner,
+                "h2d_bytes_per_call": nbytes, "d2h_bytes_per_call": nbytes,
+                "call": "upload every field from pinned host, %d steps, download every field"
+                        % args.e2e_inner},
         "gpu_launches": launches,
         "clocks": clk,
     }

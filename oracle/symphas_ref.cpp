@@ -5,6 +5,8 @@
  */
 #include "symphas_ref.h"
 
+#include <thread>
+
 // The initial-expression registry lives in SymPhas's modules library, which
 // is not built here; no model below names an initial expression.
 template <size_t D, typename T>
@@ -78,4 +80,38 @@ int symref_rhs(const symref_desc* d, const double* fields, double* rhs) {
     return 3;
   }
 }
+
+// a model held between calls, built from the fields (interior, back to back):
+// NULL for a combination not built or a storage of other extents
+void* symref_create(const symref_desc* d, const double* fields) {
+  if (is_op(d->model)) return nullptr;
+  const symref::entry* e = find(d, true);
+  if (!e) return nullptr;
+  try {
+    return e->e_create(*d, fields);
+  } catch (const std::exception& ex) {
+    std::fprintf(stderr, "symref_create: %s\n", ex.what());
+    return nullptr;
+  }
 }
+
+void symref_step(void* h, int nsteps) { static_cast<symref::system_base*>(h)->step(nsteps); }
+
+void symref_get(void* h, double* fields) { static_cast<symref::system_base*>(h)->get(fields); }
+
+void symref_destroy(void* h) { delete static_cast<symref::system_base*>(h); }
+
+// nsteps iterations of each of `count` independent models, the models spread
+// over `threads` host threads (each model on one thread, as SymPhas runs one
+// model)
+void symref_step_many(void** hs, int count, int nsteps, int threads) {
+  if (threads < 1) threads = 1;
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t)
+    pool.emplace_back([=] {
+      for (int i = t; i < count; i += threads) symref_step(hs[i], nsteps);
+    });
+  for (auto& th : pool) th.join();
+}
+}
+

@@ -105,18 +105,21 @@ namespace symref {
 
 constexpr int BD = 3;
 
+struct system_base;
 using models_fn = int (*)(const symref_desc&, const double*, double*, int);
 using ops_fn = int (*)(const symref_desc&, const double*, double*);
+using create_fn = system_base* (*)(const symref_desc&, const double*);
 struct entry {
   int e_dim, e_acc, e_lap, e_gradlap, e_bilap;
   models_fn e_models;
   ops_fn e_ops;
+  create_fn e_create;
 };
 // every stencil a translation unit instantiated, filled at load time
 std::vector<entry>& registry();
 struct reg {
-  reg(int dim, int acc, int l, int g, int b, models_fn m, ops_fn o) {
-    registry().push_back(entry{dim, acc, l, g, b, m, o});
+  reg(int dim, int acc, int l, int g, int b, models_fn m, ops_fn o, create_fn c) {
+    registry().push_back(entry{dim, acc, l, g, b, m, o, c});
   }
 };
 
@@ -216,31 +219,80 @@ void store_fields(const symref_desc& d, M& model, double* fields, bool dframe,
      ...);
 }
 
-// steps > 0: advance the fields by that many SolverFT iterations (the loop
-// of model_iteration).  steps == 0: one update() and equation(), then the
-// right-hand side (each system's dframe) is written to out.
-template <template <size_t, typename> class MT, size_t D, typename Sp, size_t NF>
-int run(const symref_desc& d, const double* in, double* out, int steps) {
-  using model_type = MT<D, SolverFT<Sp>>;
+// A SymPhas model held between calls (bench.py's reference arm times its
+// steps without the construction): one MODEL type on one stencil, its fields
+// loaded from the caller's interior arrays.
+struct system_base {
+  virtual ~system_base() = default;
+  // advance by n SolverFT iterations (the loop of model_iteration)
+  virtual void step(int n) = 0;
+  // the fields (interior, back to back) after a last update(), as
+  // find_solution leaves them
+  virtual void get(double* out) = 0;
+  // update() and equation() once; each system's dframe into out
+  virtual void rhs(double* out) = 0;
+};
+
+inline symphas::problem_parameters_type default_params(const symref_desc& d, size_t nf) {
   params::extend_boundary = false;
-  auto pp = make_params(d, NF);
-  model_type model(d.c, 8, pp);
-  if (!load_fields<NF>(d, model, in, std::make_index_sequence<NF>{})) return 2;
+  return make_params(d, nf);
+}
+
+template <template <size_t, typename> class MT, size_t D, typename Sp, size_t NF>
+struct system : system_base {
+  using model_type = MT<D, SolverFT<Sp>>;
+  symref_desc d;
+  symphas::problem_parameters_type pp;
+  model_type model;
   double t = 0.0;
-  if (steps == 0) {
+  bool ok;
+
+  system(const symref_desc& d0, const double* in)
+      : d(d0), pp(default_params(d0, NF)), model(d0.c, 8, pp) {
+    ok = load_fields<NF>(d, model, in, std::make_index_sequence<NF>{});
+  }
+  void step(int n) override {
+    for (int s = 0; s < n; ++s) {
+      model.update(t);
+      model.equation();
+      model.step(d.dt);
+      t += d.dt;
+    }
+  }
+  void get(double* out) override {
+    model.update(t);
+    store_fields(d, model, out, false, std::make_index_sequence<NF>{});
+  }
+  void rhs(double* out) override {
     model.update(t);
     model.equation();
     store_fields(d, model, out, true, std::make_index_sequence<NF>{});
-    return 0;
   }
-  for (int s = 0; s < steps; ++s) {
-    model.update(t);
-    model.equation();
-    model.step(d.dt);
-    t += d.dt;
+};
+
+template <template <size_t, typename> class MT, size_t D, typename Sp, size_t NF>
+system_base* make_system(const symref_desc& d, const double* in) {
+  auto* s = new system<MT, D, Sp, NF>(d, in);
+  if (!s->ok) {
+    delete s;
+    return nullptr;
   }
-  model.update(t);
-  store_fields(d, model, out, false, std::make_index_sequence<NF>{});
+  return s;
+}
+
+// steps > 0: advance the fields by that many SolverFT iterations.  steps ==
+// 0: one update() and equation(), then the right-hand side (each system's
+// dframe) is written to out.
+template <template <size_t, typename> class MT, size_t D, typename Sp, size_t NF>
+int run(const symref_desc& d, const double* in, double* out, int steps) {
+  system<MT, D, Sp, NF> s(d, in);
+  if (!s.ok) return 2;
+  if (steps == 0) {
+    s.rhs(out);
+  } else {
+    s.step(steps);
+    s.get(out);
+  }
   return 0;
 }
 
@@ -281,6 +333,19 @@ int gradlap_x(const symref_desc& d, const double* in, double* out) {
 }
 
 template <size_t D, typename Sp>
+system_base* create_model(const symref_desc& d, const double* in) {
+  switch (d.model) {
+    case REF_MODEL_A: return make_system<model_REFMA_t, D, Sp, 1>(d, in);
+    case REF_MODEL_B: return make_system<model_REFMB_t, D, Sp, 1>(d, in);
+    case REF_MODEL_C: return make_system<model_REFMC_t, D, Sp, 2>(d, in);
+    case REF_MODEL_AMK: return make_system<model_REFAMK_t, D, Sp, 1>(d, in);
+    case REF_MODEL_BMK: return make_system<model_REFBMK_t, D, Sp, 1>(d, in);
+    case REF_MODEL_MBB: return make_system<model_REFMBB_t, D, Sp, 1>(d, in);
+    default: return nullptr;
+  }
+}
+
+template <size_t D, typename Sp>
 int dispatch_model(const symref_desc& d, const double* in, double* out, int steps) {
   switch (d.model) {
     case REF_MODEL_A: return run<model_REFMA_t, D, Sp, 1>(d, in, out, steps);
@@ -314,4 +379,5 @@ int ops(const symref_desc& d, const double* in, double* out) {
 // stencil type, e.g. SYMREF_REGISTER(r0, 2, 2, Stencil2d2h, 5, 6, 13, 1, 1)
 #define SYMREF_REGISTER(NAME, D, ACC, SP, L, G, B, M, O)                                   \
   static symref::reg NAME(D, ACC, L, G, B, (M) ? &symref::models<D, SP<L, G, B>> : nullptr, \
-                          (O) ? &symref::ops<D, SP<L, G, B>> : nullptr);
+                          (O) ? &symref::ops<D, SP<L, G, B>> : nullptr,                     \
+                          (M) ? &symref::create_model<D, SP<L, G, B>> : nullptr);

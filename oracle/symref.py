@@ -65,3 +65,45 @@ def rhs(d, fields):
     out = np.zeros_like(a)
     _check(_need().symref_rhs(ctypes.byref(d), spo._ptr(a), spo._ptr(out)), "symref_rhs")
     return out
+
+
+class System:
+    """A SymPhas model held between calls (the reference arm of bench.py times
+    its steps): built from `fields`, stepped in place, read back."""
+
+    def __init__(self, d, fields):
+        lib = _need()
+        lib.symref_create.argtypes = [ctypes.POINTER(spo.Desc), ctypes.POINTER(ctypes.c_double)]
+        lib.symref_create.restype = ctypes.c_void_p
+        lib.symref_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.symref_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        lib.symref_destroy.argtypes = [ctypes.c_void_p]
+        self.d = d
+        a = np.ascontiguousarray(fields, dtype=np.float64)
+        self.shape = a.shape
+        self.h = lib.symref_create(ctypes.byref(d), spo._ptr(a))
+        if not self.h:
+            raise RuntimeError("symref_create: combination not built or storage mismatch")
+
+    def step(self, n=1):
+        _need().symref_step(self.h, int(n))
+
+    def get(self):
+        out = np.empty(self.shape, dtype=np.float64)
+        _need().symref_get(self.h, spo._ptr(out))
+        return out
+
+    def close(self):
+        if self.h:
+            _need().symref_destroy(self.h)
+            self.h = None
+
+
+def step_many(systems, nsteps, threads):
+    """`nsteps` iterations of every system, spread over `threads` host threads
+    (each model on one thread)."""
+    lib = _need()
+    lib.symref_step_many.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int]
+    arr = (ctypes.c_void_p * len(systems))(*[s.h for s in systems])
+    lib.symref_step_many(arr, len(systems), int(nsteps), int(threads))
