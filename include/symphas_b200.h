@@ -168,8 +168,16 @@ int sp_download(sp_handle* h, int inst, int field, void* host, size_t bytes);
 int sp_download_device(sp_handle* h, int inst, int field, void* dev, size_t bytes);
 
 /* FP64 reductions over the interior of field `field` of instance `inst`:
- * mass = sum of values, energy = h^D * sum of the model's free-energy density
- * (forward-difference gradients).  Waits for the result. */
+ * mass = sum of values (SymPhas's Density collector,
+ * dataprocesses/datadensity.h:11-19; its Energy collector is that sum over
+ * the number of sites, dataprocesses/dataenergy.h:11-19), energy = h^D * sum
+ * of a Landau free-energy density (forward-difference gradients; no SymPhas
+ * counterpart):
+ *   A, B:      -c1 v^2 / 2 + c2 v^4 / 4 + |grad v|^2 / 2
+ *   AMK, BMK:  -v^2 / 2 + v^4 / 4 + c2 |grad v|^2 / 2
+ *   C:         the same for psi and eta with unit coefficients, + c1 psi^2 eta^2
+ * The mass is not scaled by h^D.  Waits for the result; SP_ENONFINITE when a
+ * sum is NaN or infinite. */
 int sp_reduce(sp_handle* h, int inst, int field, double* mass, double* energy);
 
 /* Time every tile shape built for this kernel on this GPU (`reps` launches
@@ -251,10 +259,16 @@ int sp_adam_step(float* w, void* wb, const float* g, float* m, float* v, long lo
  * caller already holds in device memory and without a handle:
  *   fields  device pointer, `batch` instances back to back, each holding the
  *           model's fields (2 for SP_MODEL_C, else 1) as compact interiors
- *           (x-fastest, periodic on every axis), dtype SP_F32 or SP_F64;
+ *           (x-fastest, periodic on every axis), dtype SP_F32 or SP_F64:
+ *           batch * fields * n[0] * n[1] (* n[2]) elements, which the call
+ *           cannot check;
  *   out     device pointer to 2 * batch doubles: (mass of field 0, energy)
- *           per instance; written in stream order on `stream`;
- *   model, coeff, h select the free-energy density as in sp_reduce.
+ *           per instance; written in stream order on `stream`.  No host wait
+ *           is made, so a NaN or infinite sum is written as it is (sp_reduce
+ *           reports it as SP_ENONFINITE): the caller checks `out`;
+ *   model, coeff, h select the free-energy density as in sp_reduce (models
+ *           A, B, C, AMK, BMK; h positive and finite); energy is scaled by
+ *           h^D, mass is not.
  * It calls no allocator.  Its scratch is one static device array of
  * SP_NOALLOC_MAX_INSTANCES * SP_NOALLOC_BLOCKS_PER_INSTANCE * 2 doubles
  * (128 KiB) that every GPU loading this library keeps until the process exits;

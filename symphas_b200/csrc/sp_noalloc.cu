@@ -14,6 +14,7 @@
  */
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 
@@ -110,9 +111,12 @@ __global__ void __launch_bounds__(NA_THREADS) k_noalloc_finish(const NaParams p)
   }
 }
 
-// device address of the scratch array, looked up once per device
+// device address of the scratch array, looked up once per device.  Host
+// threads may make their first calls on a device at the same time: each looks
+// the address up (the runtime answers both alike) and stores it; the atomic
+// slots make those concurrent stores and loads well defined.
 constexpr int NA_MAX_DEVICES = 64;
-double* g_scratch[NA_MAX_DEVICES] = {};
+std::atomic<double*> g_scratch[NA_MAX_DEVICES] = {};
 
 int energy_kind_of(int model) {
   switch (model) {
@@ -139,11 +143,16 @@ int sp_reduce_fields_noalloc(const void* fields, int dtype, int dim, const int n
                              void* stream) {
   g_msg[0] = 0;
   if (!fields || !n || !out) return na_fail(SP_EINVAL, "null pointer argument");
+  if (model != SP_MODEL_A && model != SP_MODEL_B && model != SP_MODEL_C && model != SP_MODEL_AMK &&
+      model != SP_MODEL_BMK)
+    return na_fail(SP_EINVAL,
+                   "model must be SP_MODEL_A, SP_MODEL_B, SP_MODEL_C, SP_MODEL_AMK or SP_MODEL_BMK");
   if (dtype != SP_F32 && dtype != SP_F64) return na_fail(SP_EINVAL, "dtype must be SP_F32 or SP_F64");
   if (dim != 2 && dim != 3) return na_fail(SP_EINVAL, "dim must be 2 or 3");
   for (int a = 0; a < dim; ++a)
     if (n[a] < 1) return na_fail(SP_EINVAL, "extents must be positive");
-  if (!(h > 0.0)) return na_fail(SP_EINVAL, "grid spacing h must be positive");
+  if (!(h > 0.0) || !std::isfinite(h))
+    return na_fail(SP_EINVAL, "grid spacing h must be positive and finite");
   if (batch < 1 || batch > NA_MAX_INST) {
     char b[160];
     snprintf(b, sizeof b,
@@ -155,7 +164,8 @@ int sp_reduce_fields_noalloc(const void* fields, int dtype, int dim, const int n
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES)
     return na_fail(SP_ECUDA, "no current CUDA device");
-  if (!g_scratch[dev]) {
+  double* scratch = g_scratch[dev].load(std::memory_order_relaxed);
+  if (!scratch) {
     // first call on this device: the host-side name of the array is not a
     // device address; ask the runtime for the address on the current device
     void* ptr = nullptr;
@@ -164,7 +174,8 @@ int sp_reduce_fields_noalloc(const void* fields, int dtype, int dim, const int n
       snprintf(g_msg, sizeof g_msg, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
       return SP_ECUDA;
     }
-    g_scratch[dev] = static_cast<double*>(ptr);
+    scratch = static_cast<double*>(ptr);
+    g_scratch[dev].store(scratch, std::memory_order_relaxed);
   }
   NaParams p{};
   p.fields = fields;
@@ -178,7 +189,7 @@ int sp_reduce_fields_noalloc(const void* fields, int dtype, int dim, const int n
   p.kappa = model == SP_MODEL_C ? 1.0 : p.c2;
   p.gamma = p.c1;
   p.h = h;
-  p.partial = g_scratch[dev];
+  p.partial = scratch;
   p.out = out;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const dim3 grid(NA_BLOCKS, batch);

@@ -162,6 +162,9 @@ class Model:
     def _nbytes(self):
         return int(np.prod(self.dims)) * np.dtype(self.np_dtype).itemsize
 
+    def _inst_sites(self, inst):
+        return int(np.prod(self.dims))
+
     def set_field(self, field, values, inst=0):
         a = np.ascontiguousarray(values, dtype=self.np_dtype)
         if a.shape != self.shape:
@@ -238,12 +241,24 @@ class Model:
         C.check(C.lib().sp_conserve_mass(self._h, int(every)), self._h)
 
     def reduce(self, field=0, inst=0):
-        """(mass, free energy) in FP64."""
+        """(mass, free energy) in FP64: the sum of the field's values and h^D
+        times the sum of a Landau free-energy density (no SymPhas
+        counterpart; sp_reduce in include/symphas_b200.h gives the formula)."""
         m = ctypes.c_double()
         e = ctypes.c_double()
         C.check(C.lib().sp_reduce(self._h, inst, field, ctypes.byref(m), ctypes.byref(e)),
                 self._h)
         return m.value, e.value
+
+    def density(self, field=0, inst=0):
+        """SymPhas's Density collector (dataprocesses/datadensity.h:11-19): the
+        sum of the field's values, in FP64."""
+        return self.reduce(field, inst)[0]
+
+    def energy(self, field=0, inst=0):
+        """SymPhas's Energy collector (dataprocesses/dataenergy.h:11-19): the
+        sum of the field's values over the number of sites, in FP64."""
+        return self.reduce(field, inst)[0] * (1.0 / self._inst_sites(inst))
 
     def structure_factor(self, field=0, inst=0, threshold=True):
         """(k, S): SymPhas's radially averaged structure factor of the field
@@ -380,6 +395,9 @@ class Ensemble(Model):
 
     def _shape(self, inst):
         return tuple(reversed(self.member_dims[inst]))
+
+    def _inst_sites(self, inst):
+        return int(np.prod(self.member_dims[inst]))
 
     def sites(self):
         return sum(int(np.prod(x)) for x in self.member_dims)
