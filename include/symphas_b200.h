@@ -196,8 +196,18 @@ int sp_set_dt(sp_handle* h, double dt);
 
 /* Run all further work of the handle on `stream` (a cudaStream_t). */
 int sp_set_stream(sp_handle* h, void* stream);
-/* Wait until all queued work of the handle is done. */
+/* Wait until all queued work of the handle is done.  SP_ETIMEOUT when a
+ * kernel gave up on a bounded wait since the last check; the handle's device
+ * error flag is then cleared and its 2D work queue re-armed, so the handle
+ * stays usable. */
 int sp_synchronize(sp_handle* h);
+/* Test hook for that failure path (no counterpart in SymPhas): queue on the
+ * handle's stream one warp that waits `cycles` SM cycles (at most 2^31) on an
+ * mbarrier nothing completes -- no copy is in flight -- then gives up as a
+ * step kernel does and sets the device error flag; with `dirty_queue` it
+ * first takes an item from the handle's 2D work queue without re-arming it.
+ * The next synchronising call returns SP_ETIMEOUT. */
+int sp_test_wait_timeout(sp_handle* h, long long cycles, int dirty_queue);
 /* Number of fused-step kernel launches issued so far by this handle. */
 long long sp_launch_count(const sp_handle* h);
 /* Device pointer of the current interior origin of a field and its

@@ -1025,6 +1025,15 @@ int sp_synchronize(sp_handle* H) {
   return check_err_flag(H);
 }
 
+int sp_test_wait_timeout(sp_handle* H, long long cycles, int dirty_queue) {
+  if (!H || cycles < 0 || cycles > (1LL << 31)) return SP_EINVAL;
+  int* queue = dirty_queue ? H->ctr_d : nullptr;
+  if (dirty_queue && !queue) return fail(H, SP_EINVAL, "the handle has no 2D work queue");
+  sp::k_wait_probe<<<1, 32, 0, H->stream>>>(H->err_d, queue, cycles);
+  SP_CUDA(H, cudaGetLastError());
+  return SP_OK;
+}
+
 long long sp_launch_count(const sp_handle* H) { return H ? H->launches : -1; }
 
 int sp_field_geometry(const sp_handle* H, int inst, int field, void** dev_origin,

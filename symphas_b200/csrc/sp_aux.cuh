@@ -8,6 +8,7 @@
 #include <stdint.h>
 
 #include "sp_common.cuh"
+#include "sp_tma.cuh"
 
 namespace sp {
 
@@ -211,6 +212,23 @@ __global__ void k_mass_shift(T* base, const ShiftParams p, const double* mass,
       cell = T(u < frac ? hi : lo);
     }
   }
+}
+
+// The failure path of a step kernel, on its own: one warp waits on an
+// mbarrier that nothing will complete (no copy is in flight), gives up after
+// `limit` SM cycles as a step kernel gives up on a TMA tile, and sets the
+// device error flag.  With `queue` it first takes an item from the 2D work
+// queue and leaves without re-arming it, as a CTA that gave up mid-step does.
+__global__ void k_wait_probe(int* err, int* queue, long long limit) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    tma::mbar_init(&bar, 1);
+    tma::fence_barrier_init();
+    if (queue) atomicAdd(queue, 1);
+  }
+  __syncwarp();
+  const bool ok = tma::mbar_wait_limit(&bar, 0, limit, 20000u);
+  if (!ok && threadIdx.x == 0) atomicExch(err, KERR_TMA_TIMEOUT);
 }
 
 }  // namespace sp

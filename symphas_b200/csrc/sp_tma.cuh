@@ -63,15 +63,22 @@ __device__ __forceinline__ bool mbar_try_wait_for(uint64_t* bar, uint32_t parity
   return ok != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`: each try sleeps up to 1 ms in
-// hardware (woken when the phase completes); give up after about 2^31 SM
-// cycles (~1 s).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for phase `parity` of `bar`: each try sleeps up to `sleep_ns`
+// in hardware (woken when the phase completes); give up once more than
+// `limit` SM cycles have passed.
+__device__ __forceinline__ bool mbar_wait_limit(uint64_t* bar, uint32_t parity, long long limit,
+                                                uint32_t sleep_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  while (!mbar_try_wait_for(bar, parity, 1000000u))
-    if (clock64() - t0 > (1LL << 31)) return false;
+  while (!mbar_try_wait_for(bar, parity, sleep_ns))
+    if (clock64() - t0 > limit) return false;
   return true;
+}
+
+// The waits of the step kernels: 1 ms tries, give up after about 2^31 SM
+// cycles (~1 s).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  return mbar_wait_limit(bar, parity, 1LL << 31, 1000000u);
 }
 
 // Error path of a CTA that gave up on a wait: before it leaves, wait (again
