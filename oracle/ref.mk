@@ -1,6 +1,8 @@
 # Builds SymPhas's own CPU solver into oracle/_ref/libsymphas_ref.so, the
-# oracle's pin.  TEST INFRASTRUCTURE ONLY: tests/ and bench.py's reference arm
-# load it; the product never does.
+# oracle's pin, and oracle/_ref/symphas_binding, SymPhas's models run through
+# the SymPhas-side binding of the B200 library (symphas_b200/binding/) beside
+# SymPhas's CPU solver.  TEST INFRASTRUCTURE ONLY: tests/ and bench.py's
+# reference arm use them; the product never does.
 #
 #   make -f ref.mk [REF=<SymPhas source dir>]
 #
@@ -32,10 +34,12 @@ REF_SRCS := $(filter-out %/colormap.cpp %xdr.cpp,$(foreach m,$(MODULES),$(wildca
 REF_OBJS := $(foreach m,$(MODULES),$(patsubst $(REF)/$(m)/src/%.cpp,$(OBJ)/$(m)_%.o,$(filter $(REF)/$(m)/src/%,$(REF_SRCS))))
 DRV_SRCS := symphas_ref.cpp ref_models_2d.cpp ref_models_3d.cpp ref_ops_2d.cpp ref_ops_3d.cpp
 DRV_OBJS := $(patsubst %.cpp,$(OBJ)/drv_%.o,$(DRV_SRCS))
+BINDING := $(OUT)/symphas_binding
+B200_LIB := ../symphas_b200/lib/libsymphas_b200.so
 GEN_H := $(GEN)/configured-defs.h
 HDRS := ref_shim.h $(GEN_H)
 
-all: $(LIB)
+all: $(LIB) $(BINDING)
 
 $(GEN_H): ref_configure.py
 	$(PY) ref_configure.py $(REF) $(GEN)
@@ -54,6 +58,15 @@ $(OBJ)/drv_%.o: %.cpp symphas_ref.h $(HDRS) | $(OBJ)
 
 $(LIB): $(DRV_OBJS) $(REF_OBJS)
 	$(CXX) -shared -o $@ $^ -lpthread
+
+$(OBJ)/binding_test.o: ../tests/cpp/symphas_binding.cpp ../symphas_b200/binding/solverftb200.h \
+                       ../include/symphas_b200.h $(HDRS) | $(OBJ)
+	$(CXX) $(CXXFLAGS) $(INC) -I../include -c $< -o $@
+
+# the B200 library is found next to the package at run time ($ORIGIN-relative)
+$(BINDING): $(OBJ)/binding_test.o $(REF_OBJS) $(B200_LIB)
+	$(CXX) -o $@ $(OBJ)/binding_test.o $(REF_OBJS) -L../symphas_b200/lib -lsymphas_b200 \
+	  -Wl,-rpath,'$$ORIGIN/../../symphas_b200/lib' -lpthread
 
 endif
 
