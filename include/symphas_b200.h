@@ -248,6 +248,17 @@ int sp_conv3x3_fwd(const void* x, const void* w, const float* bias, const void* 
 int sp_conv3x3_fwd_tc(const void* x, const void* w, const float* bias, const void* res, void* z,
                       void* a, int n, int h, int w_, int cin, int cout, void* stream);
 int sp_conv_tc_status(int* gave_up);
+/* The same convolution on tcgen05 with every input pixel gathered once: the
+ * input staged as a strip of circularly padded positions (one 16-byte row per
+ * position and 8-channel chunk), the nine taps as start-address offsets of
+ * the MMA operand, four 128-position accumulators per CTA in tensor memory,
+ * the weights re-tiled into `wt` (9 cin cout bf16 of scratch, device memory)
+ * and loaded with one bulk copy per channel block.  cin a multiple of 16,
+ * cout 32, 64 or a multiple of 128, w_ <= 764; bounded waits report through
+ * sp_conv_tc_status. */
+int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, const float* bias,
+                         const void* res, void* z, void* a, int n, int h, int w_, int cin,
+                         int cout, void* stream);
 /* dw [cout][3][3][cin] (fp32) += weight gradient of that convolution for the
  * output gradient dy [n][h][w][cout]; cin a multiple of 32, cout of 8. */
 int sp_conv3x3_wgrad(const void* x, const void* dy, float* dw, int n, int h, int w_, int cin,

@@ -707,3 +707,323 @@ extern "C" int sp_conv3x3_fwd_tc(const void* x, const void* w, const float* bias
   if (cout % 128 == 0) return launch_fwd_tc<128>(p, err, s);
   return launch_fwd_tc<64>(p, err, s);
 }
+
+// ---------------------------------------------------------------------------
+// The forward convolution on tcgen05 with every input pixel gathered once.
+//
+// The input is staged as a strip of the PADDED position space: position
+// Q = (n (H + 2) + y + 1) (W + 2) + x + 1 holds pixel (n, y mod H, x mod W)
+// (circular padding), so a 3x3 tap (dy, dx) is the constant offset
+// dy (W + 2) + dx between positions.  In shared memory the strip is
+// chunk-major: for each 8-channel chunk, one 16-byte row per position.  In the
+// K-major canonical layout without swizzle that is a stack of 8-row x 16-byte
+// core matrices, 128 B apart along M (SBO) and P x 16 B apart along K (LBO,
+// P = positions in the strip); the A operand of tap t is then the same strip
+// with its start address moved by 16 x offset(t) bytes.  Each input value is
+// copied into shared memory once per channel block instead of nine times.
+//
+// A CTA owns MT = 4 M-tiles of 128 consecutive padded positions (halo
+// positions compute values nobody stores) and BN output channels; its fp32
+// accumulators (MT x BN columns) sit in tensor memory.  K runs over channel
+// blocks of CB input channels (stages): per stage the producers (warps 0-7)
+// gather the strip with 16-byte cp.async, one of them loads the stage's
+// pre-tiled weights with one bulk copy; one thread of warp 8 issues the
+// 9 x CB/16 x MT MMAs (M 128, N BN, K 16) and commits them to the stage's
+// empty barrier.  After the last stage warps 0-7 read the accumulators back
+// (tcgen05.ld) for the bias / residual / GELU epilogue.
+// ---------------------------------------------------------------------------
+namespace sp {
+namespace conv {
+
+struct StripParams {
+  const __nv_bfloat16* x;    // [N][H][W][Cin]
+  const __nv_bfloat16* wt;   // weights tiled for the stages (k_tile_weights)
+  const float* bias;         // [Cout] or null
+  const __nv_bfloat16* res;  // [N][H][W][Cout] or null
+  __nv_bfloat16* z;          // pre-activation out, or null
+  __nv_bfloat16* a;          // gelu(z) out, or null
+  int n, h, wid, cin, cout;
+  int P;                     // positions of the strip (multiple of 8)
+  int S;                     // stages in the ring
+};
+
+constexpr int ST_MT = 4, ST_M = ST_MT * 128, ST_NPROD = 256, ST_NT = ST_NPROD + 32;
+constexpr int ST_NPI = 8;  // strip positions per producer thread, at most
+
+template <int BN, int CB>
+struct StripTile {
+  static constexpr int CH = CB / 8;
+  static constexpr int B_BYTES = BN * 9 * CB * 2;
+  static constexpr int COLS = ST_MT * BN;  // 128, 256 or 512: powers of two
+  static_assert(COLS == 128 || COLS == 256 || COLS == 512, "tensor memory columns");
+  static_assert(CB % 16 == 0 && BN % 16 == 0 && BN <= 128, "tile");
+};
+
+// wt, per (output block of BN channels, input block of CB channels), in the
+// K-major canonical layout the MMA reads: [n group of 8 channels][K chunk
+// (tap-major, 8 input channels)][8 rows x 16 B]
+__global__ void k_tile_weights(const __nv_bfloat16* w, __nv_bfloat16* wt, int cin, int cout,
+                               int bn, int cb) {
+  const long long total = 9LL * cin * cout;
+  const int nkb = cin / cb, kch = 9 * cb / 8;
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+       id += (long long)gridDim.x * blockDim.x) {
+    const int ci = int(id % cin), t = int((id / cin) % 9), co = int(id / (9LL * cin));
+    const int cob = co / bn, g = (co % bn) / 8, r = co % 8;
+    const int kb = ci / cb, j = (ci % cb) / 8, e = ci % 8;
+    const int kc = t * (cb / 8) + j;
+    const long long blk = (long long)(cob * nkb + kb) * bn * 9 * cb;
+    wt[blk + ((long long)g * kch + kc) * 64 + r * 8 + e] = w[id];
+  }
+}
+
+__device__ __forceinline__ uint64_t umma_desc_k(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  // K-major, no swizzle: start, leading (K) and stride (M/N) byte offsets, >> 4
+  return uint64_t((saddr >> 4) & 0x3FFF) | (uint64_t((lbo >> 4) & 0x3FFF) << 16) |
+         (uint64_t((sbo >> 4) & 0x3FFF) << 32) | (uint64_t(1) << 46);
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <int BN, int CB>
+__global__ void __launch_bounds__(ST_NT) k_conv3x3_strip(const StripParams p, int* err) {
+  using TT = StripTile<BN, CB>;
+  constexpr int CH = TT::CH;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int S = p.S, P = p.P;
+  const int A_BYTES = CH * P * 16;
+  const int STAGE = A_BYTES + TT::B_BYTES;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * STAGE);
+  uint64_t* empty = full + S;
+  uint64_t* done = empty + S;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int W2 = p.wid + 2, H2 = p.h + 2;
+  const long long HW2 = (long long)W2 * H2, QN = HW2 * p.n;
+  const long long Q0 = (long long)blockIdx.x * ST_M;  // first output position
+  const long long S0 = Q0 - (W2 + 1);                 // first strip position
+  const int co0 = blockIdx.y * BN;
+  const int nk = p.cin / CB;
+
+  if (warp == 8) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(TT::COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      tma::mbar_init(&full[s], ST_NPROD + 1);
+      tma::mbar_init(&empty[s], 1);
+    }
+    tma::mbar_init(done, 1);
+    tma::fence_barrier_init();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  bool bad = false;
+
+  if (warp < 8) {
+    // producer: strip positions tid + 256 i; the element offset of each
+    // position's pixel (channel 0), or -1 for zeros (outside the batch)
+    int off[ST_NPI];
+#pragma unroll
+    for (int i = 0; i < ST_NPI; ++i) {
+      const int pos = tid + ST_NPROD * i;
+      const long long q = S0 + pos;
+      off[i] = -2;  // no such strip position
+      if (pos < P) {
+        off[i] = -1;
+        if (q >= 0 && q < QN) {
+          const long long nn = q / HW2, r = q - nn * HW2;
+          int yy = int(r / W2) - 1, xx = int(r % W2) - 1;
+          yy += yy < 0 ? p.h : 0;
+          yy -= yy >= p.h ? p.h : 0;
+          xx += xx < 0 ? p.wid : 0;
+          xx -= xx >= p.wid ? p.wid : 0;
+          off[i] = int(((nn * p.h + yy) * p.wid + xx) * p.cin);
+        }
+      }
+    }
+    for (int ks = 0; ks < nk && !bad; ++ks) {
+      const int s = ks % S;
+      if (ks >= S && !tma::mbar_wait(&empty[s], uint32_t((ks / S - 1) & 1))) {
+        bad = true;
+        break;
+      }
+      unsigned char* sa = smem + s * STAGE;
+      if (tid == 0) {
+        tma::mbar_arrive_expect_tx(&full[s], uint32_t(TT::B_BYTES));
+        bulk_load(sa + A_BYTES,
+                  p.wt + (long long)(blockIdx.y * nk + ks) * (TT::B_BYTES / 2),
+                  uint32_t(TT::B_BYTES), &full[s]);
+      }
+      const int c0 = ks * CB;
+#pragma unroll
+      for (int i = 0; i < ST_NPI; ++i) {
+        if (off[i] == -2) continue;
+        const int pos = tid + ST_NPROD * i;
+        const __nv_bfloat16* src = p.x + (off[i] >= 0 ? off[i] + c0 : 0);
+#pragma unroll
+        for (int j = 0; j < CH; ++j)
+          cp_async16(sa + (j * P + pos) * 16, src + j * 8, off[i] >= 0);
+      }
+      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(
+                       smem_u32(&full[s]))
+                   : "memory");
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+
+    // epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. + 31 of the
+    // M-tiles m = w / 4, w / 4 + 2
+    bad |= !tma::mbar_wait(done, 0);
+    __syncwarp();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int lq = 32 * (warp & 3);
+    for (int m = warp >> 2; m < ST_MT; m += 2) {
+      const long long q = Q0 + m * 128 + lq + lane;
+      const long long nn = q / HW2, r = q - nn * HW2;
+      const int yp = int(r / W2), xp = int(r % W2);
+      const bool store = !bad && q < QN && yp >= 1 && yp <= p.h && xp >= 1 && xp <= p.wid;
+      const long long pix = (nn * p.h + (yp - 1)) * p.wid + (xp - 1);
+#pragma unroll
+      for (int c16 = 0; c16 < BN / 16; ++c16) {
+        uint32_t v[16];
+        tmem_ld16(tmem + (uint32_t(lq) << 16) + uint32_t(m * BN + c16 * 16), v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (store) {
+          const int cob = co0 + c16 * 16;
+          const long long o = pix * p.cout + cob;
+          __align__(16) __nv_bfloat162 zz[8], aa[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            float v0 = __uint_as_float(v[2 * e]), v1 = __uint_as_float(v[2 * e + 1]);
+            if (p.bias) {
+              v0 += p.bias[cob + 2 * e];
+              v1 += p.bias[cob + 2 * e + 1];
+            }
+            if (p.res) {
+              const __nv_bfloat162 rr =
+                  *reinterpret_cast<const __nv_bfloat162*>(p.res + o + 2 * e);
+              v0 += __bfloat162float(rr.x);
+              v1 += __bfloat162float(rr.y);
+            }
+            zz[e] = __floats2bfloat162_rn(v0, v1);
+            if (p.a) aa[e] = __floats2bfloat162_rn(gelu(v0), gelu(v1));
+          }
+          if (p.z) {
+            reinterpret_cast<uint4*>(p.z + o)[0] = reinterpret_cast<const uint4*>(zz)[0];
+            reinterpret_cast<uint4*>(p.z + o)[1] = reinterpret_cast<const uint4*>(zz)[1];
+          }
+          if (p.a) {
+            reinterpret_cast<uint4*>(p.a + o)[0] = reinterpret_cast<const uint4*>(aa)[0];
+            reinterpret_cast<uint4*>(p.a + o)[1] = reinterpret_cast<const uint4*>(aa)[1];
+          }
+        }
+      }
+    }
+  } else if (lane == 0) {
+    // MMA issuer: per stage, for every tap and K step of 16 channels, one MMA
+    // per M-tile
+    constexpr uint32_t idesc = umma_idesc<BN>();
+    const uint32_t lbo = uint32_t(P * 16), sbo_b = uint32_t(9 * CB / 8 * 128);
+    for (int ks = 0; ks < nk; ++ks) {
+      const int s = ks % S;
+      if (!tma::mbar_wait(&full[s], uint32_t((ks / S) & 1))) {
+        bad = true;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(smem + s * STAGE);
+      const uint32_t b0 = a0 + uint32_t(A_BYTES);
+#pragma unroll 1
+      for (int t = 0; t < 9; ++t) {
+        const int offp = (t / 3 - 1) * W2 + (t % 3 - 1) + (W2 + 1);  // strip row of M row 0
+#pragma unroll
+        for (int kk = 0; kk < CB / 16; ++kk) {
+          const uint64_t bd = umma_desc_k(b0 + uint32_t((t * CH + 2 * kk) * 128), 128u, sbo_b);
+#pragma unroll
+          for (int m = 0; m < ST_MT; ++m) {
+            const uint64_t ad =
+                umma_desc_k(a0 + uint32_t((2 * kk * P + offp + m * 128) * 16), lbo, 128u);
+            umma_bf16(tmem + uint32_t(m * BN), ad, bd, idesc,
+                      (ks > 0 || t > 0 || kk > 0) ? 1u : 0u);
+          }
+        }
+      }
+      umma_commit(&empty[s]);
+    }
+    umma_commit(done);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 8)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TT::COLS));
+  if (bad) atomicExch(err, 1);
+}
+
+template <int BN, int CB>
+int launch_strip(StripParams p, int* err, cudaStream_t s) {
+  using TT = StripTile<BN, CB>;
+  const int W2 = p.wid + 2;
+  p.P = ((ST_M + 2 * (W2 + 1)) + 7) / 8 * 8;
+  if (p.P > ST_NPROD * ST_NPI) return SP_EINVAL;  // rows wider than the producers cover
+  const int stage = TT::CH * p.P * 16 + TT::B_BYTES;
+  const int nk = p.cin / CB;
+  const int budget = 227 * 1024 - 1024;
+  int S = budget / stage;
+  if (S < 1) return SP_EINVAL;
+  S = S < nk ? S : nk;
+  S = S < 4 ? S : 4;
+  p.S = S;
+  int smem = S * stage + (2 * S + 1) * 8 + 16;
+  // 512 tensor-memory columns leave no room for a second CTA on the SM: ask
+  // for enough shared memory that only one is resident
+  if (TT::COLS == 512 && smem < 116 * 1024) smem = 116 * 1024;
+  const cudaError_t attr = cudaFuncSetAttribute(
+      k_conv3x3_strip<BN, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (attr != cudaSuccess) return SP_ECUDA;
+  const long long QN = (long long)(p.h + 2) * W2 * p.n;
+  k_conv3x3_strip<BN, CB><<<dim3(unsigned((QN + ST_M - 1) / ST_M), unsigned(p.cout / BN)), ST_NT,
+                            smem, s>>>(p, err);
+  return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ECUDA;
+}
+
+}  // namespace conv
+}  // namespace sp
+
+extern "C" int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, const float* bias,
+                                    const void* res, void* z, void* a, int n, int h, int w_,
+                                    int cin, int cout, void* stream) {
+  using namespace sp::conv;
+  if (!x || !w || !wt || (!z && !a) || n < 1 || h < 1 || w_ < 1 || cin % 16 != 0 ||
+      !(cout == 32 || cout == 64 || cout % 128 == 0))
+    return SP_EINVAL;
+  // (n (h + 2) + h + 1) (w + 2) + ... stays an int offset per pixel
+  if ((long long)n * h * w_ * cin >= (1LL << 31)) return SP_EINVAL;
+  int* err = tc_error_flag();
+  if (!err) return SP_ENOMEM;
+  const int bn = cout == 32 ? 32 : cout == 64 ? 64 : 128;
+  const int cb = cin % 32 == 0 && cin <= 64 ? 32 : 16;
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  k_tile_weights<<<256, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(w),
+                                      static_cast<__nv_bfloat16*>(wt), cin, cout, bn, cb);
+  if (cudaGetLastError() != cudaSuccess) return SP_ECUDA;
+  StripParams p{static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(wt),
+                bias, static_cast<const __nv_bfloat16*>(res), static_cast<__nv_bfloat16*>(z),
+                static_cast<__nv_bfloat16*>(a), n, h, w_, cin, cout, 0, 0};
+  if (bn == 32) return cb == 32 ? launch_strip<32, 32>(p, err, s) : launch_strip<32, 16>(p, err, s);
+  if (bn == 64) return cb == 32 ? launch_strip<64, 32>(p, err, s) : launch_strip<64, 16>(p, err, s);
+  return cb == 32 ? launch_strip<128, 32>(p, err, s) : launch_strip<128, 16>(p, err, s);
+}

@@ -48,17 +48,27 @@ def _ok(rc, what):
         raise C.SymPhasError(rc, what)
 
 
-# True: forward convolutions on the tcgen05 kernel (tensor-memory accumulator)
-# where its shapes allow (cin % 8 == 0, cout 32 or a multiple of 64).  Off by
-# default: its im2col gather re-reads each input pixel once per tap, and on the
-# network's shapes it runs at 54-171 TFLOP/s against the mma.sync kernel's
-# 72-190, so mma.sync stays the default.
-USE_TC = False
+# The forward convolutions (and the data gradients, forward convolutions of
+# the flipped weights) run on
+#   "strip"  the tcgen05 kernel that stages each input pixel once and reads the
+#            nine taps as operand offsets (sp_conv3x3_fwd_strip), where its
+#            shapes allow (cin % 16 == 0, cout 32, 64 or a multiple of 128,
+#            width <= 764), else on the next;
+#   "tc"     the tcgen05 kernel with a per-tap gather (sp_conv3x3_fwd_tc);
+#   "mma"    the mma.sync kernel (sp_conv3x3_fwd).
+KERNEL = "strip"
 
 
-def _fwd(x, wb, bias, res, z, a, ci, co):
+def _strip_ok(ci, co, w):
+    return ci % 16 == 0 and (co in (32, 64) or co % 128 == 0) and w <= 764
+
+
+def _fwd(x, wb, bias, res, z, a, ci, co, scratch=None):
     n, h, w = x.shape[:3]
-    if USE_TC and ci % 8 == 0 and (co == 32 or co % 64 == 0):
+    if KERNEL == "strip" and scratch is not None and _strip_ok(ci, co, w):
+        _ok(C.lib().sp_conv3x3_fwd_strip(_p(x), _p(wb), _p(scratch), _p(bias), _p(res), _p(z),
+                                         _p(a), n, h, w, ci, co, _s()), "sp_conv3x3_fwd_strip")
+    elif KERNEL in ("strip", "tc") and ci % 8 == 0 and (co == 32 or co % 64 == 0):
         _ok(C.lib().sp_conv3x3_fwd_tc(_p(x), _p(wb), _p(bias), _p(res), _p(z), _p(a), n, h, w,
                                       ci, co, _s()), "sp_conv3x3_fwd_tc")
     else:
@@ -77,6 +87,8 @@ class ConvLayer:
         self.b = torch.zeros(cout, device="cuda")
         self.wb = self.w.bfloat16()
         self.wf = torch.empty(cin, 3, 3, cout, device="cuda", dtype=torch.bfloat16)
+        # the weights (or the flipped weights) re-tiled for the strip kernel
+        self.wt = torch.empty(9 * cin * cout, device="cuda", dtype=torch.bfloat16)
         self.gw = torch.zeros_like(self.w)
         self.gb = torch.zeros_like(self.b)
         self.m = [torch.zeros_like(self.w), torch.zeros_like(self.b)]
@@ -109,7 +121,7 @@ class _Conv(torch.autograd.Function):
     def forward(ctx, x, anchor, layer, res):
         n, h, w, ci = x.shape
         z = torch.empty(n, h, w, layer.cout, device="cuda", dtype=torch.bfloat16)
-        _fwd(x, layer.wb, layer.b, res, z, None, ci, layer.cout)
+        _fwd(x, layer.wb, layer.b, res, z, None, ci, layer.cout, layer.wt)
         ctx.save_for_backward(x)
         ctx.layer = layer
         ctx.has_res = res is not None
@@ -128,7 +140,7 @@ class _Conv(torch.autograd.Function):
         if ctx.needs_input_grad[0]:
             _ok(C.lib().sp_conv3x3_flip(_p(L.wb), _p(L.wf), ci, L.cout, _s()), "sp_conv3x3_flip")
             dx = torch.empty_like(x)
-            _fwd(dz, L.wf, None, None, dx, None, L.cout, ci)
+            _fwd(dz, L.wf, None, None, dx, None, L.cout, ci, L.wt)
         return dx, None, None, (dz if ctx.has_res else None)
 
 
@@ -147,7 +159,7 @@ def conv_gelu(x, layer, res=None):
         return gelu(conv(x, layer, res))
     n, h, w, ci = x.shape
     a = torch.empty(n, h, w, layer.cout, device="cuda", dtype=torch.bfloat16)
-    _fwd(x, layer.wb, layer.b, res, None, a, ci, layer.cout)
+    _fwd(x, layer.wb, layer.b, res, None, a, ci, layer.cout, layer.wt)
     return a
 
 

@@ -93,7 +93,8 @@ def test_tc_forward_rejects_unsupported_shapes():
                                      stream()) == C.SP_EINVAL
 
 
-def test_surrogate_network_on_either_kernel():
+@pytest.mark.parametrize("kernel", ["tc", "strip"])
+def test_surrogate_network_on_either_kernel(kernel):
     """The jump network gives the same prediction with its forward
     convolutions on tcgen05 or on mma.sync (bf16 activations: 2e-2)."""
     from symphas_b200 import surrogate as S
@@ -101,14 +102,62 @@ def test_surrogate_network_on_either_kernel():
     torch.cuda.set_device(0)
     net = S.JumpNet((32, 64, 128))
     psi = torch.rand(2, 64, 64, device="cuda") - 0.5
-    old = S.USE_TC
+    old = S.KERNEL
     try:
         with torch.no_grad():
-            S.USE_TC = False
+            S.KERNEL = "mma"
             d0 = net(psi)
-            S.USE_TC = True
+            S.KERNEL = kernel
             d1 = net(psi)
     finally:
-        S.USE_TC = old
+        S.KERNEL = old
     assert status() == 0
     assert rel(d1, d0) < 2e-2
+
+
+@pytest.mark.parametrize("n,h,w,ci,co", [(2, 16, 24, 32, 64), (1, 9, 7, 64, 32),
+                                         (1, 8, 8, 128, 256), (3, 33, 17, 32, 32),
+                                         (1, 10, 10, 16, 128), (2, 64, 64, 64, 128),
+                                         (1, 40, 256, 32, 32), (4, 32, 32, 256, 256)])
+def test_strip_forward_matches_reference_and_mma_sync(n, h, w, ci, co):
+    """The gather-once kernel: padded-position strip, taps as operand offsets,
+    pre-tiled weights by bulk copy -- ragged position counts, every channel
+    block size (16 and 32 input channels per stage, 1 to 16 stages), every
+    output block (32, 64, 128 channels), rows as wide as the network's 256."""
+    torch.manual_seed(1)
+    x = torch.randn(n, h, w, ci, device="cuda").bfloat16()
+    wt = (torch.randn(co, 3, 3, ci, device="cuda") / (3 * ci ** 0.5)).bfloat16()
+    b = torch.randn(co, device="cuda") * 0.1
+    res = torch.randn(n, h, w, co, device="cuda").bfloat16()
+    scratch = torch.empty(9 * ci * co, device="cuda", dtype=torch.bfloat16)
+    z = torch.full((n, h, w, co), float("nan"), device="cuda", dtype=torch.bfloat16)
+    a = torch.full_like(z, float("nan"))
+    rc = C.lib().sp_conv3x3_fwd_strip(ptr(x), ptr(wt), ptr(scratch), ptr(b), ptr(res), ptr(z),
+                                      ptr(a), n, h, w, ci, co, stream())
+    assert rc == C.SP_OK
+    assert status() == 0
+    zr = ref_conv(x.float(), wt.float(), b) + res.float()
+    assert not torch.isnan(z).any() and not torch.isnan(a).any()
+    assert rel(z.float(), zr) < 1.5e-2
+    assert rel(a.float(), F.gelu(zr, approximate="tanh")) < 1.5e-2
+    if ci % 32 == 0:
+        z2 = torch.empty_like(z)
+        assert C.lib().sp_conv3x3_fwd(ptr(x), ptr(wt), ptr(b), ptr(res), ptr(z2), None, n, h, w,
+                                      ci, co, stream()) == C.SP_OK
+        torch.cuda.synchronize()
+        assert rel(z.float(), z2.float()) < 2.0 ** -7
+
+
+def test_strip_forward_rejects_unsupported_shapes():
+    x = torch.zeros(1, 4, 800, 32, device="cuda", dtype=torch.bfloat16)
+    wt = torch.zeros(64, 3, 3, 32, device="cuda", dtype=torch.bfloat16)
+    s = torch.zeros(9 * 32 * 64, device="cuda", dtype=torch.bfloat16)
+    z = torch.zeros(1, 4, 800, 64, device="cuda", dtype=torch.bfloat16)
+    # too wide a row for the strip, an input channel count not a multiple of 16,
+    # an output block the kernel does not build
+    assert C.lib().sp_conv3x3_fwd_strip(ptr(x), ptr(wt), ptr(s), None, None, ptr(z), None, 1, 4,
+                                        800, 32, 64, stream()) == C.SP_EINVAL
+    assert C.lib().sp_conv3x3_fwd_strip(ptr(x), ptr(wt), ptr(s), None, None, ptr(z), None, 1, 4,
+                                        4, 24, 64, stream()) == C.SP_EINVAL
+    assert C.lib().sp_conv3x3_fwd_strip(ptr(x), ptr(wt), ptr(s), None, None, ptr(z), None, 1, 4,
+                                        4, 32, 96, stream()) == C.SP_EINVAL
