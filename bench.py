@@ -21,6 +21,19 @@ advanced by one step, summed over instances):
   c3d       model C (psi conserved, eta not, gamma 0.5), 8 instances of 256^3
             periodic, dx 1, dt 0.005, FP32 fused, psi_bar 0.1 +- 0.1 and eta
             +-0.1; one launch advances all 8 (2.1 GB per buffer, beyond L2).
+  surrogate the metric's second half: time to t_end of the judged learned jump
+            against plain FD on the same GPU.  2D model B 256^2 periodic, dx 1,
+            dt 0.01, Stencil2d2h<5,6,13>, psi_bar U[-0.4,0.4] +- 0.1, 2000 FD
+            steps of warm-up; a batch of 256 fields (the configuration's
+            inference batch) advanced to t_end = 6 intervals of 1000 + 4 steps,
+            by FP32 fused FD alone and by the network (jumps of 1000 steps,
+            tcgen05 convolutions, each jump judged by 4 FD steps, falling back
+            to FD when judged off the solution manifold).  The network is
+            trained first (256 FD trajectories, 20 snapshots each, Adam) unless
+            --surrogate-load names saved weights.  value = effective
+            site-updates/s of the surrogate path (t_end steps x sites / its
+            time); the FD rate, the ratio and the relative L2 error at t_end
+            are in the line.
   regional  model B 2D on a regional system (SymPhas's SolverSystemFDwSD):
             one droplet of radius 200 in a 4096^2 periodic domain, FP32 fused,
             dt 0.01; the window (about 1/15 of the domain) is re-centred every
@@ -69,7 +82,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="b3d", choices=["b3d", "ensemble", "c3d", "regional"])
+    ap.add_argument("--workload", default="b3d",
+                    choices=["b3d", "ensemble", "c3d", "regional", "surrogate"])
+    ap.add_argument("--surrogate-load", default="",
+                    help="surrogate: weights of a trained jump network (else it is trained first)")
+    ap.add_argument("--surrogate-train-steps", type=int, default=6000)
     ap.add_argument("--dtype", default="f32", choices=["f32", "f64"],
                     help="b3d only: FP32 fused step (default) or the FP64 exact step")
     ap.add_argument("--e2e-inner", type=int, default=100,
@@ -526,6 +543,63 @@ def run_reference(args):
     return 0
 
 
+def run_surrogate(args):
+    """The surrogate workload (see the module docstring): one JSON line."""
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    from symphas_b200 import surrogate as S
+
+    n, jump, warm, batch, intervals, judge = 256, 1000, 2000, 256, 6, 4
+    net = S.JumpNet((32, 64, 128, 256))
+    trained = {}
+    if args.surrogate_load:
+        net.load(torch.load(args.surrogate_load))
+        trained = {"weights": os.path.basename(args.surrogate_load)}
+    else:
+        t0 = time.perf_counter()
+        snaps = S.trajectories(256, 20, jump, n, 0.01, seed=1, warm=warm)
+        hist = S.train(net, snaps, args.surrogate_train_steps, 32, 1e-3, log=lambda *_: None)
+        torch.cuda.synchronize()
+        trained = {"trajectories": 256, "pairs": 256 * 20, "adam_steps": args.surrogate_train_steps,
+                   "train_s": round(time.perf_counter() - t0, 1), "final_loss": hist[-1][1]}
+        del snaps
+    ev = S.evaluate(net, batch=batch, jumps=intervals, jump=jump, judge_steps=judge, dt=0.01,
+                    warm=warm, n=n, threshold=3.0)
+    if rank != 0:
+        return 0
+    sites = float(batch * n * n * ev["t_end_steps"])
+    value = sites / (ev["surrogate_ms"] * 1e-3)
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": intervals,
+        "warmup": 1, "ms_per_step": ev["surrogate_ms"] / intervals, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16 network, f32 FD", "data": "synthetic",
+        "config": {"workload": "learned jump (model B 2D 256^2, batch 256, jumps of 1000 steps "
+                               "judged by 4 FD steps) to t_end = %d steps against plain FP32 "
+                               "fused FD" % ev["t_end_steps"],
+                   "fd_site_updates_per_s": sites / (ev["fd_ms"] * 1e-3),
+                   "speedup_vs_fd": ev["speedup"], "rel_l2_mean": ev["rel_l2_mean"],
+                   "rel_l2_max": ev["rel_l2_max"], "fallback_intervals": ev["fallback_intervals"],
+                   "net_ms_per_jump": ev["net_ms_per_jump"], "net_tflops": ev["net_tflops"],
+                   "training": trained},
+        "roofline": {"bound": "tensor", "achieved": ev["net_tflops"],
+                     "peak": measured_tensor_peak()[0], "unit": "TFLOP/s",
+                     "frac": ev["net_tflops"] / measured_tensor_peak()[0],
+                     "peak_kind": measured_tensor_peak()[1],
+                     "kernel": "the jump network's convolutions (sp_conv3x3_fwd_strip)"},
+    }))
+    return 0
+
+
+def measured_tensor_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]), \
+            "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
 def run_ours(args):
     import torch
 
@@ -682,6 +756,13 @@ def run_ours(args):
     return 0
 def main():
     args = parse()
+    if args.workload == "surrogate":
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the learned jump has no counterpart in SymPhas"}))
+            return 0
+        return run_surrogate(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
