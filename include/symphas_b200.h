@@ -181,10 +181,18 @@ int sp_download_device(sp_handle* h, int inst, int field, void* dev, size_t byte
 int sp_reduce(sp_handle* h, int inst, int field, double* mass, double* energy);
 
 /* Time every tile shape built for this kernel on this GPU (`reps` launches
- * each, evaluating the right-hand side so the fields are not changed) and keep
- * the fastest; later sp_create calls with the same kernel and size in the same
+ * each, per step; the fields are not changed: one-step kernels evaluate the
+ * right-hand side, temporally blocked ones write their steps into the buffer
+ * that is not current) and keep the fastest, which fixes the temporal-block
+ * depth too; later sp_create calls with the same kernel and size in the same
  * process start with it.  No counterpart in SymPhas. */
 int sp_autotune(sp_handle* h, int reps);
+/* Steps one launch of the chosen kernel advances (its temporal-block depth):
+ * 1 for the one-step kernels; k > 1 for a temporally blocked 2D kernel, which
+ * sp_step then launches once per k steps (and once with fewer steps for a
+ * remainder).  No counterpart in SymPhas (SolverFT takes one step per call of
+ * Solver::step, examples/solvers/solverft.h:46-103). */
+int sp_steps_per_launch(const sp_handle* h, int* kt);
 /* The chosen kernel shape: {tile x, tile y, rows per thread, TMA stages in
  * flight, variant index, number of variants, threads per CTA, z planes per
  * CTA (3D) or persistent CTAs (2D)}. */

@@ -98,6 +98,7 @@ SIGNATURES = {
                                  ctypes.POINTER(ctypes.c_double)]),
     "sp_autotune": (ctypes.c_int, [_H, ctypes.c_int]),
     "sp_kernel_info": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
+    "sp_steps_per_launch": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "sp_test_wait_timeout": (ctypes.c_int, [_H, ctypes.c_longlong, ctypes.c_int]),
     "sp_set_stream": (ctypes.c_int, [_H, _P]),
     "sp_set_dt": (ctypes.c_int, [_H, ctypes.c_double]),

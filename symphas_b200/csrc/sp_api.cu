@@ -159,8 +159,11 @@ int check_err_flag(sp_handle* H) {
   return SP_OK;
 }
 
+// one launch of the configured kernel: `steps` steps (1 unless the kernel is
+// temporally blocked; then at most its kt), from the current buffer into the
+// other; `advance` false leaves the current buffer current (timing runs)
 template <class T>
-int launch_step_t(sp_handle* H, int rhs_only, double* partial) {
+int launch_step_t(sp_handle* H, int rhs_only, double* partial, int steps, bool advance) {
   const int src = H->cur, dst = H->cur ^ 1;
   const double divh = 1.0 / H->d.h;
   const double divh2 = divh * divh, divh3 = divh * divh2, divh4 = divh2 * divh2;
@@ -201,17 +204,21 @@ int launch_step_t(sp_handle* H, int rhs_only, double* partial) {
     p.hy = H->h[1];
     p.partial = partial;
     p.err = H->err_d;
+    p.in = reinterpret_cast<const T* const*>(H->outs_d[src]);
+    p.tsteps = steps;
     e = H->ki->launch(&p, dim3(H->grid2), H->stream);
   }
   if (e != cudaSuccess) return cuda_fail(H, e, "fused step launch");
   ++H->launches;
-  if (!rhs_only) H->cur = dst;
+  if (!rhs_only && advance) H->cur = dst;
   return SP_OK;
 }
 
-int launch_step(sp_handle* H, int rhs_only, double* partial) {
-  return H->esz == 4 ? launch_step_t<float>(H, rhs_only, partial)
-                     : launch_step_t<double>(H, rhs_only, partial);
+int launch_step(sp_handle* H, int rhs_only, double* partial, int steps = 1, bool advance = true) {
+  if (steps < 1 || steps > H->ki->kt || (rhs_only && steps != 1))
+    return fail(H, SP_EINVAL, "steps per launch outside the kernel's range");
+  return H->esz == 4 ? launch_step_t<float>(H, rhs_only, partial, steps, advance)
+                     : launch_step_t<double>(H, rhs_only, partial, steps, advance);
 }
 
 template <class T>
@@ -364,6 +371,14 @@ int setup_2d_t(sp_handle* H) {
 // instance to be a 3D grid of their x extent, periodic in x)
 bool applicable(const sp_handle* H, int v) {
   const sp::KernelInfo& k = H->variants[v];
+  if (k.kt > 1) {
+    // temporally blocked: 2D, periodic on both axes, x extents in whole copies
+    if (H->dim != 2) return false;
+    for (int s = 0; s < 4; ++s)
+      if (H->d.boundary[s] != SP_PERIODIC) return false;
+    for (const InstGeo& g : H->geo)
+      if (g.n[0] % k.x_multiple != 0) return false;
+  }
   if (k.nx_only == 0) return true;
   if (H->dim != 3 || H->d.boundary[0] != SP_PERIODIC) return false;
   for (const InstGeo& g : H->geo)
@@ -667,7 +682,7 @@ int capture_graph(sp_handle* H) {
   }
   int rc = SP_OK;
   const long long before = H->launches;
-  for (int i = 0; i < GRAPH_STEPS && rc == SP_OK; ++i) rc = launch_step(H, 0, nullptr);
+  for (int i = 0; i < GRAPH_STEPS && rc == SP_OK; ++i) rc = launch_step(H, 0, nullptr, H->ki->kt);
   cudaError_t e = cudaStreamEndCapture(H->stream, &g);
   H->launches = before;
   H->cur = parity;
@@ -862,16 +877,19 @@ int sp_conserve_mass(sp_handle* H, int every) {
 
 namespace {
 int step_plain(sp_handle* H, int nsteps) {
+  // a graph replays GRAPH_STEPS launches of kt steps each
+  const int kt = H->ki->kt, chunk = GRAPH_STEPS * kt;
   while (nsteps > 0) {
-    if (nsteps >= GRAPH_STEPS && H->graphs && !H->gexec[H->cur])
+    if (nsteps >= chunk && H->graphs && !H->gexec[H->cur])
       if (int rc = capture_graph(H)) return rc;
-    if (nsteps >= GRAPH_STEPS && H->gexec[H->cur]) {
+    if (nsteps >= chunk && H->gexec[H->cur]) {
       SP_CUDA(H, cudaGraphLaunch(H->gexec[H->cur], H->stream));
       H->launches += GRAPH_STEPS;
-      nsteps -= GRAPH_STEPS;
+      nsteps -= chunk;
     } else {
-      if (int rc = launch_step(H, 0, nullptr)) return rc;
-      --nsteps;
+      const int s = std::min(kt, nsteps);
+      if (int rc = launch_step(H, 0, nullptr, s)) return rc;
+      nsteps -= s;
     }
   }
   return SP_OK;
@@ -937,11 +955,15 @@ int sp_autotune(sp_handle* H, int reps) {
   for (int v = 0; v < int(H->variants.size()) && rc == SP_OK; ++v) {
     if (!applicable(H, v)) continue;
     if ((rc = configure(H, v))) break;
-    // right-hand-side launches: the same loads and stores as a step, and the
-    // state of the model is left untouched
-    for (int i = 0; i < 2 && rc == SP_OK; ++i) rc = launch_step(H, 1, nullptr);
+    // one-step kernels: right-hand-side launches, the same loads and stores
+    // as a step; temporally blocked ones: launches of kt whole steps into the
+    // other buffer, which is not made current.  Either leaves the state of
+    // the model untouched; the time is taken per step.
+    const int kt = H->ki->kt;
+    auto once = [&]() { return kt > 1 ? launch_step(H, 0, nullptr, kt, false) : launch_step(H, 1, nullptr); };
+    for (int i = 0; i < 2 && rc == SP_OK; ++i) rc = once();
     cudaEventRecord(e0, H->stream);
-    for (int i = 0; i < reps && rc == SP_OK; ++i) rc = launch_step(H, 1, nullptr);
+    for (int i = 0; i < reps && rc == SP_OK; ++i) rc = once();
     cudaEventRecord(e1, H->stream);
     if (rc) break;
     if (cudaEventSynchronize(e1) != cudaSuccess) {
@@ -950,6 +972,7 @@ int sp_autotune(sp_handle* H, int reps) {
     }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
+    ms /= float(kt);
     if (ms < best_ms) {
       best_ms = ms;
       best = v;
@@ -965,6 +988,12 @@ int sp_autotune(sp_handle* H, int reps) {
     g_tuned[tune_key(H)] = best;
   }
   return check_err_flag(H);
+}
+
+int sp_steps_per_launch(const sp_handle* H, int* kt) {
+  if (!H || !kt) return SP_EINVAL;
+  *kt = H->ki->kt;
+  return SP_OK;
 }
 
 int sp_kernel_info(const sp_handle* H, int info[8]) {

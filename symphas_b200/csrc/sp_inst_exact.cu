@@ -85,5 +85,12 @@ void register_exact_kernels() {
   SP_EXACT_SET(float, 0, 9, 6, 13, 15, 10, 25)
   SP_OPS2(double, 1)
   SP_OPS3(double, 1)
+  // temporally blocked FP64 shapes (sp_tb2.cuh), two steps per launch: the
+  // same bits as two one-step launches
+  SP_REG2TB(SPK_A, SPK_EXACT, MF_A_exact, MF_A_exact, double, 1, 5, 6, 13, ::sp::Tiles<double>::T2a);
+  SP_REG2TB(SPK_B, SPK_EXACT, MF_B_exact, MF_B_exact, double, 1, 5, 6, 13, ::sp::Tiles<double>::T2a);
+  SP_REG2TB(SPK_C, SPK_EXACT, MF_C_exact, MF_C_exact, double, 1, 5, 6, 13, ::sp::Tiles<double>::T2a);
+  SP_REG2TB(SPK_ENS_AB, SPK_EXACT, MF_AMK_exact, MF_BMK_exact, double, 1, 5, 6, 13,
+            ::sp::Tiles<double>::T2a);
 }
 }  // namespace sp

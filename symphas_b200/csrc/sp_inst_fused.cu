@@ -38,6 +38,11 @@
   SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3d);        \
   SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3e);        \
   SP_REG3T(MODEL, SPK_FUSED, MF, float, 0, 7, 10, 25, ::sp::Tiles<float>::D3f);
+// temporally blocked shapes (sp_tb2.cuh) of the FP32 2D fused kernels, for
+// sp_autotune: the depth is part of the shape
+#define SP_FUSED_TB2(MODEL, MF0, MF1)                                                   \
+  SP_REG2TB(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::T2a);  \
+  SP_REG2TB(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::T2b);
 #define SP_FUSED_VARIANTS2(MODEL, MF0, MF1)                                             \
   SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2b);   \
   SP_REG2T(MODEL, SPK_FUSED, MF0, MF1, float, 0, 5, 6, 13, ::sp::Tiles<float>::D2c);
@@ -59,5 +64,11 @@ void register_fused_kernels() {
   SP_FUSED_VARIANTS2(SPK_A, MF_A_fused, MF_A_fused)
   SP_FUSED_VARIANTS2(SPK_B, MF_B_fused, MF_B_fused)
   SP_FUSED_VARIANTS2(SPK_ENS_AB, MF_AMK_fused, MF_BMK_fused)
+  SP_FUSED_TB2(SPK_A, MF_A_fused, MF_A_fused)
+  SP_FUSED_TB2(SPK_B, MF_B_fused, MF_B_fused)
+  SP_FUSED_TB2(SPK_C, MF_C_fused, MF_C_fused)
+  SP_FUSED_TB2(SPK_AMK, MF_AMK_fused, MF_AMK_fused)
+  SP_FUSED_TB2(SPK_BMK, MF_BMK_fused, MF_BMK_fused)
+  SP_FUSED_TB2(SPK_ENS_AB, MF_AMK_fused, MF_BMK_fused)
 }
 }  // namespace sp

@@ -80,6 +80,10 @@ struct Step2Params {
   int hx, hy;       // common halo of every instance
   double* partial;  // per-CTA FP64 sum of the new field 0 (single instance), or null
   int* err;
+  // temporally blocked kernels (sp_tb2.cuh): input padded origins,
+  // [inst * nf + f], and the steps of this launch (1 .. the kernel's KT)
+  const T* const* in;
+  int tsteps;
 };
 
 // ---------------------------------------------------------------------------

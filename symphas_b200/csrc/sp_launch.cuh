@@ -10,6 +10,7 @@
 #include "sp_row.cuh"
 #include "sp_kernels.cuh"
 #include "sp_models.cuh"
+#include "sp_tb2.cuh"
 #include "sp_registry.h"
 
 namespace sp {
@@ -196,6 +197,39 @@ struct Entry2 {
   }
 };
 
+// the temporally blocked 2D step (sp_tb2.cuh): up to TC::KT steps per launch
+template <class MF0, class MF1, class T, int LP, int GP, int BP, class TC, bool EXACT>
+struct Entry2T {
+  using M0 = model_of<MF0>;
+  using M1 = model_of<MF1>;
+  using K = Fd2T<M0, M1, T, LP, GP, BP, TC, EXACT>;
+  static cudaError_t launch(const void* prm, dim3 grid, cudaStream_t s) {
+    auto kern = k_fd2t<M0, M1, T, LP, GP, BP, TC, EXACT>;
+    static cudaError_t attr = cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
+    if (attr != cudaSuccess) return attr;
+    const M0 m0 = MF0{}();
+    const M1 m1 = MF1{}();
+    return launch_step_kernel(kern, grid, K::NT, K::SMEM, s,
+                              *static_cast<const Step2Params<T>*>(prm), m0, m1);
+  }
+  static int occupancy() {
+    auto kern = k_fd2t<M0, M1, T, LP, GP, BP, TC, EXACT>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::SMEM));
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, K::NT, K::SMEM) != cudaSuccess)
+      return 1;
+    return n > 0 ? n : 1;
+  }
+  static KernelInfo info() {
+    KernelInfo i{K::NF, K::NS, K::R, K::HXA, K::TX, K::TY, 1, 0, K::NT, K::SMEM,
+                 &launch, &occupancy};
+    i.kt = K::KT;
+    i.x_multiple = K::LC;
+    return i;
+  }
+};
+
 // model factories
 #define SP_FACTORY(NAME, EXPR)                          \
   struct NAME {                                         \
@@ -279,10 +313,14 @@ template <> struct Tiles<float> {
   // fewer tiles in flight, less shared memory: more CTAs per SM
   using D2d = TileCfg<128, 16, 4, 2, 2>;
   using D2e = TileCfg<128, 16, 4, 1, 2>;
+  // temporally blocked 2D tiles (sp_tb2.cuh): up to 2 and 4 steps per launch
+  using T2a = TbCfg<128, 32, 2, 256, 4>;
+  using T2b = TbCfg<128, 32, 4, 256, 4>;
 };
 template <> struct Tiles<double> {
   using D3 = TileCfg<64, 16, 2, 3, 2>;
   using D2 = TileCfg<64, 16, 4, 3, 2>;
+  using T2a = TbCfg<64, 32, 2, 256, 2>;
 };
 }  // namespace sp
 
@@ -307,6 +345,9 @@ template <> struct Tiles<double> {
 #define SP_REG2T(MODEL, FORM, MF0, MF1, T, DT, LP, GP, BP, TILE)            \
   ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 2, DT, LP, GP, BP},    \
                         ::sp::Entry2<::sp::MF0, ::sp::MF1, T, LP, GP, BP, TILE, FORM == SPK_EXACT>::info())
+#define SP_REG2TB(MODEL, FORM, MF0, MF1, T, DT, LP, GP, BP, TILE)           \
+  ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 2, DT, LP, GP, BP},    \
+                        ::sp::Entry2T<::sp::MF0, ::sp::MF1, T, LP, GP, BP, TILE, FORM == SPK_EXACT>::info())
 #define SP_REG2X(MODEL, FORM, MF0, MF1, T, DT, LP, GP, BP)                 \
   ::sp::register_kernel(::sp::KernelKey{MODEL, FORM, 2, DT, LP, GP, BP},    \
                         ::sp::Entry2<::sp::MF0, ::sp::MF1, T, LP, GP, BP, ::sp::Tiles<T>::D2, FORM == SPK_EXACT>::info())

@@ -43,6 +43,11 @@ struct KernelInfo {
   int box_hx = -1;
   // nonzero: the kernel runs only on 3D grids of this x extent, periodic in x
   int nx_only = 0;
+  // steps one launch can advance (temporally blocked kernels: > 1); such a
+  // kernel runs only on 2D grids periodic on both axes whose x extents are
+  // multiples of x_multiple
+  int kt = 1;
+  int x_multiple = 1;
 };
 
 // appends a tile variant for `key` (the first registered is the default)

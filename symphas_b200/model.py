@@ -283,7 +283,11 @@ class Model:
         C.check(C.lib().sp_kernel_info(self._h, v), self._h)
         keys = ("tile_x", "tile_y", "rows_per_thread", "stages_in_flight", "variant",
                 "variants", "threads", "z_per_cta_or_ctas")
-        return dict(zip(keys, v[:]))
+        info = dict(zip(keys, v[:]))
+        kt = ctypes.c_int(0)
+        C.check(C.lib().sp_steps_per_launch(self._h, ctypes.byref(kt)), self._h)
+        info["steps_per_launch"] = kt.value
+        return info
 
     def synchronize(self):
         C.check(C.lib().sp_synchronize(self._h), self._h)
