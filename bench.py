@@ -25,12 +25,13 @@ advanced by one step, summed over instances):
             against plain FD on the same GPU.  2D model B 256^2 periodic, dx 1,
             dt 0.01, Stencil2d2h<5,6,13>, psi_bar U[-0.4,0.4] +- 0.1, 2000 FD
             steps of warm-up; a batch of 256 fields (the configuration's
-            inference batch) advanced to t_end = 6 intervals of 1000 + 4 steps,
-            by FP32 fused FD alone and by the network (jumps of 1000 steps,
-            tcgen05 convolutions, each jump judged by 4 FD steps, falling back
-            to FD when judged off the solution manifold).  The network is
-            trained first (256 FD trajectories, 20 snapshots each, Adam) unless
-            --surrogate-load names saved weights.  value = effective
+            inference batch) advanced to t_end = 3 intervals of 2000 + 4 steps,
+            by FP32 fused FD alone and by the network (jumps of 2000 steps,
+            --surrogate-jump; tcgen05 convolutions; each member's jump judged
+            by 4 FD steps, the members judged off the solution manifold
+            redone by FD).  The network is trained first (256 FD
+            trajectories, 10 snapshots each, Adam) unless --surrogate-load
+            names saved weights.  value = effective
             site-updates/s of the surrogate path (t_end steps x sites / its
             time); the FD rate, the ratio and the relative L2 error at t_end
             are in the line.
@@ -87,6 +88,13 @@ def parse():
     ap.add_argument("--surrogate-load", default="",
                     help="surrogate: weights of a trained jump network (else it is trained first)")
     ap.add_argument("--surrogate-train-steps", type=int, default=6000)
+    ap.add_argument("--surrogate-save", default="",
+                    help="surrogate: write the trained weights here (torch.save)")
+    ap.add_argument("--surrogate-jump", type=int, default=2000,
+                    help="surrogate: FD steps per learned jump (t_end stays about 6000 steps)")
+    ap.add_argument("--surrogate-trajectories", type=int, default=256)
+    ap.add_argument("--surrogate-snapshots", type=int, default=10,
+                    help="surrogate: training snapshots per trajectory, one jump apart")
     ap.add_argument("--dtype", default="f32", choices=["f32", "f64"],
                     help="b3d only: FP32 fused step (default) or the FP64 exact step")
     ap.add_argument("--e2e-inner", type=int, default=100,
@@ -551,7 +559,10 @@ def run_surrogate(args):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     from symphas_b200 import surrogate as S
 
-    n, jump, warm, batch, intervals, judge = 256, 1000, 2000, 256, 6, 4
+    n, warm, batch, judge = 256, 2000, 256, 4
+    jump = args.surrogate_jump
+    intervals = max(2, 6000 // jump)
+    ntraj, nsnap = args.surrogate_trajectories, args.surrogate_snapshots
     net = S.JumpNet((32, 64, 128, 256))
     trained = {}
     if args.surrogate_load:
@@ -559,12 +570,15 @@ def run_surrogate(args):
         trained = {"weights": os.path.basename(args.surrogate_load)}
     else:
         t0 = time.perf_counter()
-        snaps = S.trajectories(256, 20, jump, n, 0.01, seed=1, warm=warm)
+        snaps = S.trajectories(ntraj, nsnap, jump, n, 0.01, seed=1, warm=warm)
         hist = S.train(net, snaps, args.surrogate_train_steps, 32, 1e-3, log=lambda *_: None)
         torch.cuda.synchronize()
-        trained = {"trajectories": 256, "pairs": 256 * 20, "adam_steps": args.surrogate_train_steps,
+        trained = {"trajectories": ntraj, "pairs": ntraj * nsnap,
+                   "adam_steps": args.surrogate_train_steps,
                    "train_s": round(time.perf_counter() - t0, 1), "final_loss": hist[-1][1]}
         del snaps
+        if args.surrogate_save:
+            torch.save(net.state(), args.surrogate_save)
     ev = S.evaluate(net, batch=batch, jumps=intervals, jump=jump, judge_steps=judge, dt=0.01,
                     warm=warm, n=n, threshold=3.0)
     if rank != 0:
@@ -575,12 +589,16 @@ def run_surrogate(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": intervals,
         "warmup": 1, "ms_per_step": ev["surrogate_ms"] / intervals, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16 network, f32 FD", "data": "synthetic",
-        "config": {"workload": "learned jump (model B 2D 256^2, batch 256, jumps of 1000 steps "
+        "config": {"workload": "learned jump (model B 2D 256^2, batch 256, jumps of %d steps "
                                "judged by 4 FD steps) to t_end = %d steps against plain FP32 "
-                               "fused FD" % ev["t_end_steps"],
+                               "fused FD" % (jump, ev["t_end_steps"]),
                    "fd_site_updates_per_s": sites / (ev["fd_ms"] * 1e-3),
                    "speedup_vs_fd": ev["speedup"], "rel_l2_mean": ev["rel_l2_mean"],
                    "rel_l2_max": ev["rel_l2_max"], "fallback_intervals": ev["fallback_intervals"],
+                   "member_fallbacks": ev["member_fallbacks"],
+                   "fallback_members_per_interval": ev["fallback_members_per_interval"],
+                   "ms_network": ev["ms_network"], "ms_judge": ev["ms_judge"],
+                   "ms_fallback_fd": ev["ms_fallback_fd"],
                    "net_ms_per_jump": ev["net_ms_per_jump"], "net_tflops": ev["net_tflops"],
                    "training": trained},
         "roofline": {"bound": "tensor", "achieved": ev["net_tflops"],

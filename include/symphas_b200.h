@@ -262,8 +262,8 @@ int sp_conv_tc_status(int* gave_up);
  * the MMA operand, four 128-position accumulators per CTA in tensor memory,
  * the weights re-tiled into `wt` (9 cin cout bf16 of scratch, device memory)
  * and loaded with one bulk copy per channel block.  cin a multiple of 16,
- * cout 32, 64 or a multiple of 128, w_ <= 764; bounded waits report through
- * sp_conv_tc_status. */
+ * cout 32, 64 or a multiple of 128, w_ <= 764, bias 16-byte aligned; bounded
+ * waits report through sp_conv_tc_status. */
 int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, const float* bias,
                          const void* res, void* z, void* a, int n, int h, int w_, int cin,
                          int cout, void* stream);

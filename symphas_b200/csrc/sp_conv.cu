@@ -56,9 +56,19 @@ __device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4],
       : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
+// gelu, tanh form, with the hardware tanh (tanh.approx.f32, about 2^-11
+// relative): the activations are stored in bf16 (2^-8), so the result is the
+// same function to within storage rounding, for a fraction of the epilogue's
+// instructions
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ float gelu(float z) {
   const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
-  return 0.5f * z * (1.0f + tanhf(u));
+  const float hz = 0.5f * z;
+  return fmaf(hz, tanh_fast(u), hz);
 }
 
 struct FwdParams {
@@ -904,12 +914,18 @@ __global__ void __launch_bounds__(ST_NT) k_conv3x3_strip(const StripParams p, in
           const int cob = co0 + c16 * 16;
           const long long o = pix * p.cout + cob;
           __align__(16) __nv_bfloat162 zz[8], aa[8];
+          __align__(16) float bs[16];
+          if (p.bias) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              reinterpret_cast<float4*>(bs)[j] = __ldg(reinterpret_cast<const float4*>(p.bias + cob) + j);
+          }
 #pragma unroll
           for (int e = 0; e < 8; ++e) {
             float v0 = __uint_as_float(v[2 * e]), v1 = __uint_as_float(v[2 * e + 1]);
             if (p.bias) {
-              v0 += p.bias[cob + 2 * e];
-              v1 += p.bias[cob + 2 * e + 1];
+              v0 += bs[2 * e];
+              v1 += bs[2 * e + 1];
             }
             if (p.res) {
               const __nv_bfloat162 rr =
@@ -1010,6 +1026,8 @@ extern "C" int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, cons
   if (!x || !w || !wt || (!z && !a) || n < 1 || h < 1 || w_ < 1 || cin % 16 != 0 ||
       !(cout == 32 || cout == 64 || cout % 128 == 0))
     return SP_EINVAL;
+  // the epilogue reads the bias 16 channels (64 bytes) at a time
+  if (bias && reinterpret_cast<uintptr_t>(bias) % 16 != 0) return SP_EINVAL;
   // (n (h + 2) + h + 1) (w + 2) + ... stays an int offset per pixel
   if ((long long)n * h * w_ * cin >= (1LL << 31)) return SP_EINVAL;
   int* err = tc_error_flag();

@@ -297,9 +297,13 @@ def trajectories(ntraj, nsnap, jump=100, n=256, dt=0.01, seed=1, warm=0):
 # ---------------------------------------------------------------------------
 # training
 # ---------------------------------------------------------------------------
-def train(net, snaps, steps=2000, batch=32, lr=1e-3, seed=0, log_every=200, log=print):
+def train(net, snaps, steps=2000, batch=32, lr=1e-3, seed=0, log_every=200, log=print,
+          warmup=0.05, clip=1.0):
     """Fit delta = psi(t + jump) - psi(t) over all snapshot pairs (MSE on the
-    scaled change); cosine learning-rate decay."""
+    scaled change): Adam with a linear warm-up over the first `warmup`
+    fraction of the steps, cosine decay after it, and the gradients clipped to
+    a global norm of `clip` (an occasional large batch gradient otherwise
+    throws the encoder-decoder off for good)."""
     ntraj, ns1, n, _ = snaps.shape
     pairs = ntraj * (ns1 - 1)
     d = snaps[:, 1:] - snaps[:, :-1]
@@ -317,7 +321,18 @@ def train(net, snaps, steps=2000, batch=32, lr=1e-3, seed=0, log_every=200, log=
         pred = net(x)
         loss = ((pred - y) ** 2).mean() / (net.scale ** 2)
         loss.backward()
-        lr_t = lr * 0.5 * (1 + math.cos(math.pi * step / steps))
+        if clip:
+            # on the device: no host wait per step
+            sq = torch.zeros((), device="cuda")
+            for l in layers:
+                sq = sq + (l.gw * l.gw).sum() + (l.gb * l.gb).sum()
+            f = torch.clamp(clip / (sq.sqrt() + 1e-12), max=1.0)
+            for l in layers:
+                l.gw.mul_(f)
+                l.gb.mul_(f)
+        nw = max(1, int(warmup * steps))
+        lr_t = (lr * step / nw if step <= nw else
+                lr * 0.5 * (1 + math.cos(math.pi * (step - nw) / max(1, steps - nw))))
         for l in layers:
             l.adam(step, lr_t)
         if step % log_every == 0 or step == steps:
@@ -329,20 +344,61 @@ def train(net, snaps, steps=2000, batch=32, lr=1e-3, seed=0, log_every=200, log=
 # ---------------------------------------------------------------------------
 # inference: jumps judged by the FD solver
 # ---------------------------------------------------------------------------
+class FdPool:
+    """FD models of 1, 2, 4, ... instances (up to `batch`), on which the
+    intervals of the members the judge rejects are redone: each member of a
+    batch is judged on its own, and only the rejected ones pay for plain FD
+    (padded to the next pool size)."""
+
+    def __init__(self, n, batch, dt):
+        self.n, self.dt, self.batch = n, dt, batch
+        self.models = {}
+
+    def get(self, count):
+        size = 1
+        while size < count:
+            size *= 2
+        size = min(size, max(self.batch, count))
+        if size not in self.models:
+            self.models[size] = fd_model(self.n, size, self.dt)
+        return self.models[size], size
+
+    def warm(self, steps):
+        """Create every size and run `steps` steps on each (graph capture)."""
+        size = 1
+        while True:
+            m, got = self.get(size)
+            m.step(self.dt, steps)
+            if got >= self.batch:
+                break
+            size = got * 2
+
+    def close(self):
+        for m in self.models.values():
+            m.close()
+        self.models = {}
+
+
 @torch.no_grad()
-def rollout(net, psi0, jumps, jump=100, judge_steps=4, dt=0.01, threshold=3.0, m=None):
+def rollout(net, psi0, jumps, jump=100, judge_steps=4, dt=0.01, threshold=3.0, m=None,
+            pool=None, stats=None):
     """Advance psi0 [B, n, n] by `jumps` intervals of jump + judge_steps FD
     steps each.  Per interval: one network jump, then judge_steps FD steps
-    from the jumped field.  How far those FD steps move the field is its rate
-    of relaxation; under model B it only slows down as domains coarsen, so a
-    jump whose rate exceeds `threshold` times the rate before the jump (or is
-    not finite) left the solution manifold, and the interval is redone by
-    plain FD.  Returns the final field and the number of intervals that fell
-    back."""
+    from the jumped field.  How far those FD steps move a member's field is
+    its rate of relaxation; under model B it only slows down as domains
+    coarsen, so a jump whose rate exceeds `threshold` times the member's rate
+    before the jump (or is not finite) left the solution manifold, and that
+    member's interval is redone by plain FD (on a pool model of the rejected
+    members only).  Returns the final field and the number of intervals in
+    which some member fell back; `stats` (a dict), if given, receives the
+    number of member-intervals that fell back."""
     b, n, _ = psi0.shape
     own = m is None
     if own:
         m = fd_model(n, b, dt)
+    own_pool = pool is None
+    if own_pool:
+        pool = FdPool(n, b, dt)
 
     def norm(x):
         return x.flatten(1).norm(dim=1)
@@ -351,25 +407,55 @@ def rollout(net, psi0, jumps, jump=100, judge_steps=4, dt=0.01, threshold=3.0, m
     put_batch(m, psi)
     m.step(dt, judge_steps)
     rate = norm(get_batch(m, b, n) - psi)
-    fallbacks = 0
+    fallbacks, members, sizes = 0, 0, []
+    timed = stats is not None
+    ev = []
+
+    def mark():
+        if timed:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record()
+            ev.append(e)
+
     for _ in range(jumps):
+        mark()
         js = psi + net(psi)
+        mark()
         put_batch(m, js)
         m.step(dt, judge_steps)
         judged = get_batch(m, b, n)
         moved = norm(judged - js)
         bad = ~torch.isfinite(moved) | (moved > threshold * rate)
-        if bool(bad.any()):
+        idx = bad.nonzero().flatten()
+        mark()
+        if idx.numel():
             fallbacks += 1
-            put_batch(m, psi)
-            m.step(dt, jump)
-            start = get_batch(m, b, n)
-            m.step(dt, judge_steps)
-            judged = get_batch(m, b, n)
-            moved = norm(judged - start)
+            members += idx.numel()
+            sizes.append(int(idx.numel()))
+            fm, size = pool.get(idx.numel())
+            sub = torch.zeros(size, n, n, device="cuda")
+            sub[: idx.numel()] = psi[idx]
+            put_batch(fm, sub)
+            fm.step(dt, jump)
+            start = get_batch(fm, idx.numel(), n)
+            fm.step(dt, judge_steps)
+            redone = get_batch(fm, idx.numel(), n)
+            judged[idx] = redone
+            moved[idx] = norm(redone - start)
+        mark()
         psi, rate = judged, moved
     if own:
         m.close()
+    if own_pool:
+        pool.close()
+    if timed:
+        torch.cuda.synchronize()
+        t = [[ev[4 * j + k].elapsed_time(ev[4 * j + k + 1]) for k in range(3)] for j in range(jumps)]
+        stats["member_fallbacks"] = members
+        stats["fallback_members_per_interval"] = sizes
+        stats["ms_network"] = sum(x[0] for x in t)
+        stats["ms_judge"] = sum(x[1] for x in t)
+        stats["ms_fallback_fd"] = sum(x[2] for x in t)
     return psi, fallbacks
 
 
@@ -401,18 +487,23 @@ def evaluate(net, batch=64, jumps=10, jump=100, judge_steps=4, dt=0.01, seed=777
         m.step(dt, warm)
     psi0 = get_batch(m, batch, n)
     steps = jumps * (jump + judge_steps)
-    # warm both paths once (kernel selection, allocator)
-    rollout(net, psi0, 1, jump, judge_steps, dt, threshold, m)
+    # warm both paths once (kernel selection, allocator, the fallback pool's
+    # models and their graphs: set up once per run, not per interval)
+    pool = FdPool(n, batch, dt)
+    pool.warm(64)
+    rollout(net, psi0, 1, jump, judge_steps, dt, threshold, m, pool)
     fd_run(psi0, jump, dt, m)
+    stats = {}
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     ev[0].record()
     ref = fd_run(psi0, steps, dt, m)
     ev[1].record()
     ev[2].record()
-    sur, fb = rollout(net, psi0, jumps, jump, judge_steps, dt, threshold, m)
+    sur, fb = rollout(net, psi0, jumps, jump, judge_steps, dt, threshold, m, pool, stats)
     ev[3].record()
     torch.cuda.synchronize()
     m.close()
+    pool.close()
     t_fd, t_sur = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
     # the network alone: one jump of the batch, and its tensor-core throughput
     with torch.no_grad():
@@ -430,9 +521,37 @@ def evaluate(net, batch=64, jumps=10, jump=100, judge_steps=4, dt=0.01, seed=777
     return {"batch": batch, "t_end_steps": steps, "fd_ms": t_fd, "surrogate_ms": t_sur,
             "speedup": t_fd / t_sur, "rel_l2_mean": float(err.mean()),
             "rel_l2_max": float(err.max()), "fallback_intervals": fb, "intervals": jumps,
+            "member_fallbacks": stats["member_fallbacks"],
+            "fallback_members_per_interval": stats["fallback_members_per_interval"],
+            "ms_network": stats["ms_network"], "ms_judge": stats["ms_judge"],
+            "ms_fallback_fd": stats["ms_fallback_fd"],
             "max_mass_difference": mass, "net_ms_per_jump": t_net,
             "net_tflops": flops / (t_net * 1e-3) / 1e12,
             "fd_ms_per_jump": t_fd / jumps * jump / (jump + judge_steps)}
+
+
+def time_conv(n, side, cin, cout, reps=5):
+    """Time one forward convolution layer of the network's kind (3x3
+    circular, bias, GELU epilogue) on random BF16 data: `reps` launches after
+    two warm-up launches, CUDA events on the current stream."""
+    g = torch.Generator().manual_seed(0)
+    x = torch.randn(n, side, side, cin, generator=g).to("cuda", torch.bfloat16)
+    layer = ConvLayer(cin, cout, g)
+    z = torch.empty(n, side, side, cout, device="cuda", dtype=torch.bfloat16)
+    a = torch.empty_like(z)
+    scratch = layer.wt
+    for _ in range(2):
+        _fwd(x, layer.wb, layer.b, None, z, a, cin, cout, scratch)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        _fwd(x, layer.wb, layer.b, None, z, a, cin, cout, scratch)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    flops = 2.0 * n * side * side * cout * 9 * cin
+    return {"kernel": KERNEL if _strip_ok(cin, cout, side) else "fallback", "n": n, "side": side,
+            "cin": cin, "cout": cout, "ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
 
 
 def main(argv=None):
@@ -440,6 +559,8 @@ def main(argv=None):
     import json
 
     ap = argparse.ArgumentParser(description="train and evaluate the judged k-step jump")
+    ap.add_argument("--time-conv", type=int, nargs=4, metavar=("N", "SIDE", "CIN", "COUT"),
+                    help="only time one forward convolution layer of this shape and exit")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--ntraj", type=int, default=128, help="training trajectories")
     ap.add_argument("--nsnap", type=int, default=60, help="jumps per trajectory")
@@ -459,6 +580,9 @@ def main(argv=None):
     ap.add_argument("--load", default="", help="skip training, load weights")
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
+    if a.time_conv:
+        print(json.dumps(time_conv(*a.time_conv)))
+        return
     net = JumpNet(tuple(a.channels))
     report = {"params": net.nparams(), "channels": list(a.channels), "n": a.n, "jump": a.jump,
               "dt": a.dt, "warm": a.warm, "flops_per_sample": net.flops(a.n)}
