@@ -6,9 +6,14 @@ the time per step.  Used for timing and for profiling single launches:
     python -m symphas_b200.run --regional 200 --n 4096 --steps 8
                         (model B 2D, one droplet of that radius, regional window)
 
-Steps are launched one at a time (no CUDA graph), so a profiler sees each
-fused-step launch separately.
+Steps are launched one launch at a time (no CUDA graph), so a profiler sees
+each fused-step launch separately: one step per launch, or k for a
+temporally blocked kernel (the steps are rounded up to a multiple of k).
+
+    python -m symphas_b200.run --model A --dim 2 --n 4096 --steps 256 --every-variant
+                        (one line per tile shape and temporal-block depth)
 """
+import os
 import argparse
 import json
 import time
@@ -39,11 +44,33 @@ def main(argv=None):
                          "shrinks the window, the steps after it are timed")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the fastest tile shape first (its launches come before the steps)")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="run this tile variant (index into the kernel's shapes)")
+    ap.add_argument("--every-variant", action="store_true",
+                    help="time every tile variant of the kernel in turn, one line each")
     a = ap.parse_args(argv)
+    if a.every_variant:
+        nv = 1
+        v = 0
+        while v < nv:
+            os.environ["SP_TILE"] = str(v)
+            out = run_one(a, quiet=True)
+            nv = out["kernel"]["variants"]
+            if out["kernel"]["variant"] == v:
+                print(json.dumps(out))
+            v += 1
+        del os.environ["SP_TILE"]
+        return
+    if a.variant >= 0:
+        os.environ["SP_TILE"] = str(a.variant)
+    if a.ensemble or a.regional:
+        return run_ensemble(a) if a.ensemble else run_regional(a)
+    print(json.dumps(run_one(a)))
+
+
+def run_one(a, quiet=False):
     if a.ensemble:
-        return run_ensemble(a)
-    if a.regional:
-        return run_regional(a)
+        return run_ensemble(a, quiet)
     st = sp.Stencil2d2h(5, 6, 13) if a.dim == 2 else sp.Stencil3d2h(7, 10, 25)
     cls = MODELS[a.model]
     coeff = a.coeff or ([0.5] if a.model == "C" else [])
@@ -53,34 +80,46 @@ def main(argv=None):
     if cls.nfields > 1:
         m.fill_uniform(1, 2, -0.1, 0.1)
     info = m.autotune(5) if a.autotune else m.kernel_info()
+    kt = info["steps_per_launch"]
+    launches = -(-a.steps // kt)
+    m.step(a.dt, kt)  # warm-up launch
     m.synchronize()
+    l0 = m.launch_count()
     t0 = time.perf_counter()
-    for _ in range(a.steps):
-        m.step(a.dt, 1)
+    for _ in range(launches):
+        m.step(a.dt, kt)
     m.synchronize()
     el = time.perf_counter() - t0
-    print(json.dumps({"model": a.model, "dim": a.dim, "n": a.n, "dtype": a.dtype, "form": a.form,
-                      "steps": a.steps, "wall_ms_per_step": 1e3 * el / a.steps,
-                      "launches": m.launch_count(), "kernel": info}))
+    out = {"model": a.model, "dim": a.dim, "n": a.n, "dtype": a.dtype, "form": a.form,
+           "steps": launches * kt, "wall_ms_per_step": 1e3 * el / (launches * kt),
+           "launches": m.launch_count() - l0, "kernel": info}
     m.close()
+    return out
 
 
-def run_ensemble(a):
+def run_ensemble(a, quiet=False):
     members = sp.ensemble_members(a.ensemble, seed=20261203)
     e = sp.Ensemble(sp.SolverFT(sp.Stencil2d2h(5, 6, 13), form=a.form), members, dtype=a.dtype)
     for i in range(len(members)):
         e.fill_uniform(0, 20261203 + i, -0.1, 0.1, inst=i)
     info = e.autotune(5) if a.autotune else e.kernel_info()
+    kt = info["steps_per_launch"]
+    launches = -(-a.steps // kt)
+    e.step(kt)
     e.synchronize()
+    l0 = e.launch_count()
     t0 = time.perf_counter()
-    for _ in range(a.steps):
-        e.step(1)
+    for _ in range(launches):
+        e.step(kt)
     e.synchronize()
     el = time.perf_counter() - t0
-    print(json.dumps({"ensemble": len(members), "sites": e.sites(), "dtype": a.dtype,
-                      "form": a.form, "steps": a.steps, "wall_ms_per_step": 1e3 * el / a.steps,
-                      "launches": e.launch_count(), "kernel": info}))
+    out = {"ensemble": len(members), "sites": e.sites(), "dtype": a.dtype, "form": a.form,
+           "steps": launches * kt, "wall_ms_per_step": 1e3 * el / (launches * kt),
+           "launches": e.launch_count() - l0, "kernel": info}
     e.close()
+    if quiet:
+        return out
+    print(json.dumps(out))
 
 
 def run_regional(a):
