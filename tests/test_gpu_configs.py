@@ -127,6 +127,46 @@ def test_ensemble_1024_members_stratified_sample(form, dtype, tol):
     assert worst <= tol, worst
 
 
+@pytest.mark.parametrize("form,dtype", [("exact", "f64"), ("fused", "f32")])
+def test_ensemble_1024_members_5000_steps(form, dtype):
+    """The configuration's full length: all 1024 members advanced 5000 steps
+    of their own dt in one launch per step (graph-replayed), then the
+    stratified sample checked against the FP64 oracle, member by member: the
+    exact form bit-identical, the fused FP32 form within 5e-3 relative
+    L-infinity (printed per member: the figure the configuration asks for)."""
+    seed, steps = 20261203, 5000
+    members = sp.ensemble_members(1024, seed=seed)
+    ens = sp.Ensemble(sp.SolverFT(S2, form=form), members, dtype=dtype)
+    for i in range(len(members)):
+        ens.fill_uniform(0, seed + i, -0.1, 0.1, inst=i)
+    if form == "fused":
+        ens.autotune(3)
+    ens.step(steps)
+    sample = stratified(members)
+    descs, fields = [], []
+    for i in sample:
+        mb = members[i]
+        descs.append(spo.make_desc(2, mb["dims"], ORACLE_MODEL[mb["model"]], 1.0, mb["dt"],
+                                   coeff=mb["coeff"]))
+        fields.append(spo.seed_uniform(seed + i, -0.1, 0.1, mb["dims"][0] * mb["dims"][1]))
+    spo.run_batch(descs, fields, [steps] * len(sample), THREADS)
+    worst = 0.0
+    for i, ref in zip(sample, fields):
+        nx, ny = members[i]["dims"]
+        got = ens.get_field(0, inst=i).astype(np.float64)
+        ref = ref.reshape(ny, nx)
+        if dtype == "f64":
+            assert np.array_equal(got, ref), i
+        else:
+            e = rel_linf(got, ref)
+            print("member %d (%s %dx%d, M %.3f, kappa %.3f): FP32 vs FP64 rel L-inf %.3e"
+                  % (i, members[i]["model"], nx, ny, members[i]["coeff"][0],
+                     members[i]["coeff"][1], e))
+            worst = max(worst, e)
+    ens.close()
+    assert worst <= 5e-3, worst
+
+
 def test_model_c_8x256_batch():
     n, batch, steps = 256, 8, 5
     coeff = (0.5,)
