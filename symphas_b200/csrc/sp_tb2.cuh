@@ -34,17 +34,20 @@
 
 namespace sp {
 
-// TX x TY tile, up to KT steps per launch, NT threads, W sites per thread group
-template <int TX_, int TY_, int KT_, int NT_, int W_>
+// TX x TY tile, up to KT steps per launch, NT threads, W sites per thread
+// group, SR consecutive rows per work item (their shared neighbour rows are
+// loaded once)
+template <int TX_, int TY_, int KT_, int NT_, int W_, int SR_ = 4>
 struct TbCfg {
-  static constexpr int TX = TX_, TY = TY_, KT = KT_, NT = NT_, W = W_;
+  static constexpr int TX = TX_, TY = TY_, KT = KT_, NT = NT_, W = W_, SR = SR_;
 };
 
 template <class M0, class M1, class T, int LP, int GP, int BP, class TC, bool EXACT>
 struct Fd2T {
   static constexpr bool exact = EXACT;
   static_assert(M0::nf == M1::nf, "models of one launch share the field count");
-  static constexpr int TX = TC::TX, TY = TC::TY, KT = TC::KT, NT = TC::NT, W = TC::W;
+  static constexpr int TX = TC::TX, TY = TC::TY, KT = TC::KT, NT = TC::NT, W = TC::W,
+                       SR = TC::SR;
   static constexpr int NF = M0::nf;
   static constexpr int NS = imax(M0::ns, M1::ns);
   static constexpr int R = imax(M0::R, M1::R);
@@ -60,7 +63,10 @@ struct Fd2T {
   static constexpr int HX = ceil_to(ceil_to(HT, W) + W, LC);
   static constexpr int HY = HT;
   static constexpr int PW = TX + 2 * HX, PH = TY + 2 * HY;
-  static constexpr int PLANE = ceil_to(PW * PH, 32);
+  // SR - 1 rows below the region: the last work item of a region whose row
+  // count is not a multiple of SR reads them (and does not store its rows
+  // beyond the region)
+  static constexpr int PLANE = ceil_to(PW * (PH + SR - 1), 32);
   static constexpr int GW = PW / LC;  // copies per row
   // planes: input (two tiles, double-buffered) and the step buffer per field,
   // and the staged operands
@@ -68,6 +74,7 @@ struct Fd2T {
   // the field layout of the one-step kernels of the same key (their x halo)
   static constexpr int HXA = HaloGeom<T, W, R, NS, RS, RI>::HXA;
   static_assert(TX % W == 0 && TX % LC == 0, "whole groups and copies per tile row");
+  static_assert(SR >= 1 && TY % SR == 0, "the tile's rows split into work items");
   static_assert(W <= LC && LC % W == 0, "a group lies inside one 16-byte copy");
   static_assert(R <= W, "one extra group covers the reach of the rounded-out sites");
   static_assert(KT >= 1 && KT <= 8, "steps per launch");
@@ -102,8 +109,9 @@ template <class K, class M, class T, int LP, int GP, int BP, int HS>
 __device__ __forceinline__ void tb_stage(const M& m, const Inst2<T>& ip, const T* src, T* sb) {
   constexpr int W = K::W, PW = K::PW, PLANE = K::PLANE, NF = K::NF, NT = K::NT;
   constexpr int NS = M::ns;
-  constexpr int HG = (HS + W - 1) / W;
-  constexpr int NR = K::TY + 2 * HS, NG = K::TX / W + 2 * HG, CNT = NR * NG;
+  constexpr int HG = (HS + W - 1) / W, SR = K::SR;
+  constexpr int NR = K::TY + 2 * HS, NG = K::TX / W + 2 * HG, NRB = (NR + SR - 1) / SR,
+                CNT = NRB * NG;
   using V = vec_t<T, W>;
   using CS = Ctx<T, W, !K::exact, 2, LP, GP, BP, NF, 1, 0, PW, 1, 1, 0, PW>;
   T coef[8];
@@ -116,16 +124,23 @@ __device__ __forceinline__ void tb_stage(const M& m, const Inst2<T>& ip, const T
   c0.cf = coef;
 #pragma unroll 1
   for (int i = threadIdx.x; i < CNT; i += NT) {
-    const int r = i / NG, g = i - r * NG;
-    const int off = (r - HS + K::HY) * PW + (g - HG) * W + K::HX;
-    CS ctx = c0;
+    const int rb = i / NG, g = i - rb * NG;
+    const int off = (rb * SR - HS + K::HY) * PW + (g - HG) * W + K::HX;
+    // every row of the item before any store: the rows share loads
+    V s0[SR], s1[SR];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) ctx.fo[f][0] = src + f * PLANE + off;
-    const V s0 = eval(m.s0, ctx);
-    *reinterpret_cast<V*>(sb + off) = s0;
-    if constexpr (NS > 1) {
-      const V s1 = eval(m.s1, ctx);
-      *reinterpret_cast<V*>(sb + PLANE + off) = s1;
+    for (int k = 0; k < SR; ++k) {
+      CS ctx = c0;
+#pragma unroll
+      for (int f = 0; f < NF; ++f) ctx.fo[f][0] = src + f * PLANE + off + k * PW;
+      s0[k] = eval(m.s0, ctx);
+      if constexpr (NS > 1) s1[k] = eval(m.s1, ctx);
+    }
+#pragma unroll
+    for (int k = 0; k < SR; ++k) {
+      if (NR % SR != 0 && rb * SR + k >= NR) break;
+      *reinterpret_cast<V*>(sb + off + k * PW) = s0[k];
+      if constexpr (NS > 1) *reinterpret_cast<V*>(sb + PLANE + off + k * PW) = s1[k];
     }
   }
 }
@@ -136,8 +151,9 @@ template <class K, class M, class T, int LP, int GP, int BP, int HO>
 __device__ __forceinline__ void tb_update(const M& m, const Inst2<T>& ip, const T* src,
                                           const T* sb, T* dst) {
   constexpr int W = K::W, PW = K::PW, PLANE = K::PLANE, NF = K::NF, NT = K::NT, NS = K::NS;
-  constexpr int HG = (HO + W - 1) / W;
-  constexpr int NR = K::TY + 2 * HO, NG = K::TX / W + 2 * HG, CNT = NR * NG;
+  constexpr int HG = (HO + W - 1) / W, SR = K::SR;
+  constexpr int NR = K::TY + 2 * HO, NG = K::TX / W + 2 * HG, NRB = (NR + SR - 1) / SR,
+                CNT = NRB * NG;
   using V = vec_t<T, W>;
   using CO = Ctx<T, W, !K::exact, 2, LP, GP, BP, NF, 1, 0, PW, NS, 1, 0, PW>;
   T coef[8];
@@ -151,23 +167,31 @@ __device__ __forceinline__ void tb_update(const M& m, const Inst2<T>& ip, const 
   const V vdt(ip.dt);
 #pragma unroll 1
   for (int i = threadIdx.x; i < CNT; i += NT) {
-    const int r = i / NG, g = i - r * NG;
-    const int off = (r - HO + K::HY) * PW + (g - HG) * W + K::HX;
-    CO ctx = c0;
+    const int rb = i / NG, g = i - rb * NG;
+    const int off = (rb * SR - HO + K::HY) * PW + (g - HG) * W + K::HX;
+    V n0[SR], n1[SR];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) ctx.fo[f][0] = src + f * PLANE + off;
-    if constexpr (NS > 0) {
+    for (int k = 0; k < SR; ++k) {
+      CO ctx = c0;
 #pragma unroll
-      for (int k = 0; k < NS; ++k) ctx.so[k][0] = sb + k * PLANE + off;
+      for (int f = 0; f < NF; ++f) ctx.fo[f][0] = src + f * PLANE + off + k * PW;
+      if constexpr (NS > 0) {
+#pragma unroll
+        for (int q = 0; q < NS; ++q) ctx.so[q][0] = sb + q * PLANE + off + k * PW;
+      }
+      const V r0 = eval(m.r0, ctx);
+      n0[k] = fmadd<!K::exact>(vdt, r0, ctx.template var<1, 0, 0, 0>());
+      if constexpr (NF > 1) {
+        const V r1 = eval(m.r1, ctx);
+        n1[k] = fmadd<!K::exact>(vdt, r1, ctx.template var<2, 0, 0, 0>());
+      }
     }
-    const V r0 = eval(m.r0, ctx);
-    const V n0 = fmadd<!K::exact>(vdt, r0, ctx.template var<1, 0, 0, 0>());
-    if constexpr (NF > 1) {
-      const V r1 = eval(m.r1, ctx);
-      const V n1 = fmadd<!K::exact>(vdt, r1, ctx.template var<2, 0, 0, 0>());
-      *reinterpret_cast<V*>(dst + PLANE + off) = n1;
+#pragma unroll
+    for (int k = 0; k < SR; ++k) {
+      if (NR % SR != 0 && rb * SR + k >= NR) break;
+      *reinterpret_cast<V*>(dst + off + k * PW) = n0[k];
+      if constexpr (NF > 1) *reinterpret_cast<V*>(dst + PLANE + off + k * PW) = n1[k];
     }
-    *reinterpret_cast<V*>(dst + off) = n0;
   }
 }
 
@@ -179,7 +203,7 @@ __device__ __forceinline__ void tb_final(const Step2Params<T>& p, const M& m, co
                                          double& msum) {
   constexpr int W = K::W, PW = K::PW, PLANE = K::PLANE, NF = K::NF, NT = K::NT, NS = K::NS,
                 R = K::R, TX = K::TX, TY = K::TY;
-  constexpr int NG = TX / W, CNT = TY * NG;
+  constexpr int SR = K::SR, NG = TX / W, CNT = (TY / SR) * NG;
   using V = vec_t<T, W>;
   using CO = Ctx<T, W, !K::exact, 2, LP, GP, BP, NF, 1, 0, PW, NS, 1, 0, PW>;
   T coef[8];
@@ -206,33 +230,40 @@ __device__ __forceinline__ void tb_final(const Step2Params<T>& p, const M& m, co
   const bool rhs_only = p.rhs_only != 0;
 #pragma unroll 1
   for (int i = threadIdx.x; i < CNT; i += NT) {
-    const int r = i / NG, g = i - r * NG;
-    const int off = (r + K::HY) * PW + g * W + K::HX;
-    CO ctx = c0;
+    const int rb = i / NG, g = i - rb * NG;
+    const int off = (rb * SR + K::HY) * PW + g * W + K::HX;
+    V nv[SR][NF];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) ctx.fo[f][0] = src + f * PLANE + off;
-    if constexpr (NS > 0) {
+    for (int k = 0; k < SR; ++k) {
+      CO ctx = c0;
 #pragma unroll
-      for (int k = 0; k < NS; ++k) ctx.so[k][0] = sb + k * PLANE + off;
+      for (int f = 0; f < NF; ++f) ctx.fo[f][0] = src + f * PLANE + off + k * PW;
+      if constexpr (NS > 0) {
+#pragma unroll
+        for (int q = 0; q < NS; ++q) ctx.so[q][0] = sb + q * PLANE + off + k * PW;
+      }
+      const V r0 = eval(m.r0, ctx);
+      nv[k][0] = rhs_only ? r0 : fmadd<!K::exact>(vdt, r0, ctx.template var<1, 0, 0, 0>());
+      if constexpr (NF > 1) {
+        const V r1 = eval(m.r1, ctx);
+        nv[k][1] = rhs_only ? r1 : fmadd<!K::exact>(vdt, r1, ctx.template var<2, 0, 0, 0>());
+      }
     }
-    V nv[NF];
-    const V r0 = eval(m.r0, ctx);
-    nv[0] = rhs_only ? r0 : fmadd<!K::exact>(vdt, r0, ctx.template var<1, 0, 0, 0>());
-    if constexpr (NF > 1) {
-      const V r1 = eval(m.r1, ctx);
-      nv[1] = rhs_only ? r1 : fmadd<!K::exact>(vdt, r1, ctx.template var<2, 0, 0, 0>());
-    }
-    const int x = x0 + g * W, y = y0 + r;
-    if (plain) {
+    const int x = x0 + g * W;
 #pragma unroll
-      for (int f = 0; f < NF; ++f)
-        *reinterpret_cast<V*>(out[f] + (long long)(y + p.hy) * pitch + x + p.hx) = nv[f];
-    } else if (x < n0 && y < n1) {
+    for (int k = 0; k < SR; ++k) {
+      const int y = y0 + rb * SR + k;
+      if (plain) {
 #pragma unroll
-      for (int f = 0; f < NF; ++f)
-        store_group<T, W, 2, R>(out[f], x, y, 0, nv[f], n3, h, per3, pitch, 0);
+        for (int f = 0; f < NF; ++f)
+          *reinterpret_cast<V*>(out[f] + (long long)(y + p.hy) * pitch + x + p.hx) = nv[k][f];
+      } else if (x < n0 && y < n1) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+          store_group<T, W, 2, R>(out[f], x, y, 0, nv[k][f], n3, h, per3, pitch, 0);
+      }
+      if (p.partial && x < n0 && y < n1) msum += vsum<T, W>(nv[k][0], x, n0);
     }
-    if (p.partial && x < n0 && y < n1) msum += vsum<T, W>(nv[0], x, n0);
   }
 }
 
