@@ -166,6 +166,15 @@ int sp_eval_rhs(sp_handle* h, int inst, int field, void* host, size_t bytes);
 int sp_download(sp_handle* h, int inst, int field, void* host, size_t bytes);
 /* Same into device memory (compact interior layout), stream-ordered. */
 int sp_download_device(sp_handle* h, int inst, int field, void* dev, size_t bytes);
+/* One field of every instance at once, to or from a dense device array
+ * [instance][interior, x fastest] (`bytes` = batch x sites x element size):
+ * one copy kernel, and after an upload one halo refresh for the whole batch
+ * (periodic images, Dirichlet constants), where sp_upload_device per instance
+ * takes a copy and two halo launches each.  The instances must share their
+ * extents (a batch of one model, or an ensemble of equal members).  No
+ * counterpart in SymPhas (one host copy per system's `values`). */
+int sp_upload_batch_device(sp_handle* h, int field, const void* dev, size_t bytes);
+int sp_download_batch_device(sp_handle* h, int field, void* dev, size_t bytes);
 
 /* FP64 reductions over the interior of field `field` of instance `inst`:
  * mass = sum of values (SymPhas's Density collector,
@@ -268,7 +277,8 @@ int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, const float* bi
                          const void* res, void* z, void* a, int n, int h, int w_, int cin,
                          int cout, void* stream);
 /* dw [cout][3][3][cin] (fp32) += weight gradient of that convolution for the
- * output gradient dy [n][h][w][cout]; cin a multiple of 32, cout of 8. */
+ * output gradient dy [n][h][w][cout]; cin a multiple of 32, cout of 8, fewer
+ * than 2^31 pixels. */
 int sp_conv3x3_wgrad(const void* x, const void* dy, float* dw, int n, int h, int w_, int cin,
                      int cout, void* stream);
 /* wf [cin][3][3][cout] = w [cout][3][3][cin] rotated by 180 degrees: the input

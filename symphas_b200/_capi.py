@@ -94,6 +94,8 @@ SIGNATURES = {
     "sp_eval_rhs": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _P, _SZ]),
     "sp_download": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _P, _SZ]),
     "sp_download_device": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _P, _SZ]),
+    "sp_upload_batch_device": (ctypes.c_int, [_H, ctypes.c_int, _P, _SZ]),
+    "sp_download_batch_device": (ctypes.c_int, [_H, ctypes.c_int, _P, _SZ]),
     "sp_reduce": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                  ctypes.POINTER(ctypes.c_double)]),
     "sp_autotune": (ctypes.c_int, [_H, ctypes.c_int]),

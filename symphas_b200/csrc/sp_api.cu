@@ -246,6 +246,33 @@ int fill_halo_t(sp_handle* H, int which, int inst, int f) {
   return SP_OK;
 }
 
+// every instance's halo of field f in one launch (instances of equal extents)
+template <class T>
+int fill_halo_batch_t(sp_handle* H, int which, int f) {
+  const InstGeo& g = H->geo[0];
+  sp::HaloParams<T> p{};
+  p.org = reinterpret_cast<T*>(field_base(H, which, 0, f));
+  p.dim = H->dim;
+  for (int a = 0; a < 3; ++a) {
+    p.n[a] = g.n[a];
+    p.h[a] = H->h[a];
+  }
+  p.pitch = g.pitch;
+  p.plane = g.plane;
+  for (int s = 0; s < 6; ++s) {
+    p.bc[s] = H->d.boundary[s];
+    p.bv[s] = T(H->d.boundary_value[s]);
+  }
+  p.inst_stride = (long long)H->nf * g.felems;
+  const long long L0 = g.n[0] + 2LL * H->h[0], L1 = g.n[1] + 2LL * H->h[1];
+  const long long n2 = H->dim == 3 ? g.n[2] : 1, h2 = H->dim == 3 ? H->h[2] : 0;
+  const long long cells = 2 * h2 * L0 * L1 + n2 * 2 * H->h[1] * L0 + n2 * g.n[1] * 2 * H->h[0];
+  const int blocks = int(std::min<long long>(std::max(1LL, H->sms * 4LL / H->batch) , (cells + 255) / 256));
+  sp::k_fill_halo<T><<<dim3(std::max(blocks, 1), H->batch), 256, 0, H->stream>>>(p);
+  SP_CUDA(H, cudaGetLastError());
+  return SP_OK;
+}
+
 int fill_halo(sp_handle* H, int which, int inst, int f) {
   return H->esz == 4 ? fill_halo_t<float>(H, which, inst, f)
                      : fill_halo_t<double>(H, which, inst, f);
@@ -814,6 +841,57 @@ const char* sp_create_error(void) { return g_create_error.c_str(); }
 int sp_upload(sp_handle* h, int inst, int field, const void* host, size_t bytes) {
   if (!h || !host) return SP_EINVAL;
   return upload(h, inst, field, host, bytes, cudaMemcpyHostToDevice);
+}
+
+}  // extern "C"
+
+namespace {
+// the batch's instances share their extents and sit one after another
+bool uniform_batch(const sp_handle* H) {
+  for (int i = 0; i < H->batch; ++i) {
+    const InstGeo& g = H->geo[i];
+    for (int a = 0; a < 3; ++a)
+      if (g.n[a] != H->geo[0].n[a]) return false;
+    if (g.off != size_t(i) * H->nf * H->geo[0].felems) return false;
+  }
+  return true;
+}
+
+template <class T>
+int batch_copy_t(sp_handle* H, int field, void* dense, size_t bytes, bool to_field) {
+  if (field < 0 || field >= H->nf) return fail(H, SP_EINVAL, "field index out of range");
+  if (!uniform_batch(H))
+    return fail(H, SP_EINVAL, "batched copies need instances of equal extents");
+  const InstGeo& g = H->geo[0];
+  const long long total = (long long)H->batch * g.sites();
+  if (bytes != size_t(total) * sizeof(T))
+    return fail(H, SP_EINVAL, "byte count does not match batch x interior size");
+  const int blocks = int(std::min<long long>(H->sms * 8LL, (total + 255) / 256));
+  sp::k_batch_copy<T><<<blocks, 256, 0, H->stream>>>(
+      reinterpret_cast<T*>(field_base(H, H->cur, 0, field)), (long long)H->nf * g.felems,
+      g.pitch, g.plane, g.n[0], g.n[1], g.n[2], H->h[0], H->h[1], H->h[2],
+      static_cast<T*>(dense), total, to_field ? 1 : 0);
+  SP_CUDA(H, cudaGetLastError());
+  if (!to_field) return SP_OK;
+  // as refresh_halos, for every instance at once
+  if (int rc = fill_halo_batch_t<T>(H, H->cur ^ 1, field)) return rc;
+  return fill_halo_batch_t<T>(H, H->cur, field);
+}
+}  // namespace
+
+extern "C" {
+
+int sp_upload_batch_device(sp_handle* h, int field, const void* dev, size_t bytes) {
+  if (!h || !dev) return SP_EINVAL;
+  void* d = const_cast<void*>(dev);
+  return h->esz == 4 ? batch_copy_t<float>(h, field, d, bytes, true)
+                     : batch_copy_t<double>(h, field, d, bytes, true);
+}
+
+int sp_download_batch_device(sp_handle* h, int field, void* dev, size_t bytes) {
+  if (!h || !dev) return SP_EINVAL;
+  return h->esz == 4 ? batch_copy_t<float>(h, field, dev, bytes, false)
+                     : batch_copy_t<double>(h, field, dev, bytes, false);
 }
 
 int sp_upload_device(sp_handle* h, int inst, int field, const void* dev, size_t bytes) {

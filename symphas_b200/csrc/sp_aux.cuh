@@ -24,13 +24,15 @@ struct HaloParams {
   long long pitch, plane;
   int bc[6];
   T bv[6];
+  long long inst_stride;  // elements between instances of a batched launch (grid y)
 };
 
 // The halo cells only, enumerated as (a) the whole halo planes in z, (b) the
 // whole halo rows in y of the interior planes, (c) the halo columns in x of
 // the interior rows.
 template <class T>
-__global__ void k_fill_halo(const HaloParams<T> p) {
+__global__ void k_fill_halo(HaloParams<T> p) {
+  p.org += blockIdx.y * p.inst_stride;  // instance blockIdx.y of a batch
   const long long L0 = p.n[0] + 2 * p.h[0], L1 = p.n[1] + 2 * p.h[1];
   const int n2 = (p.dim == 3) ? p.n[2] : 1, h2 = (p.dim == 3) ? p.h[2] : 0;
   const long long A = 2LL * h2 * L0 * L1;            // halo planes
@@ -82,6 +84,27 @@ __global__ void k_fill_halo(const HaloParams<T> p) {
       w[a] = v + p.h[a];
     }
     p.org[idx] = p.org[w[2] * p.plane + w[1] * p.pitch + w[0]];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// one field of every instance of a batch (equal extents) to or from a dense
+// array [instance][z][y][x] in device memory: interiors only
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_batch_copy(T* org, long long inst_stride, long long pitch, long long plane,
+                             int n0, int n1, int n2, int h0, int h1, int h2, T* dense,
+                             long long total, int to_field) {
+  const long long sites = (long long)n0 * n1 * n2;
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+       id += (long long)gridDim.x * blockDim.x) {
+    const long long i = id / sites, s = id - i * sites;
+    const long long x = s % n0, yz = s / n0, y = yz % n1, z = yz / n1;
+    T* f = org + i * inst_stride + (z + h2) * plane + (y + h1) * pitch + (x + h0);
+    if (to_field)
+      *f = dense[id];
+    else
+      dense[id] = *f;
   }
 }
 

@@ -263,9 +263,11 @@ __global__ void __launch_bounds__(WTH) k_conv3x3_wgrad(const WgradParams p) {
       const int r = tid >> 2, ch = tid & 3;
       const long long pix = q0 + r;
       const bool ok = pix < pe;
-      const long long pp = ok ? pix : pb;
-      const int xx0 = int(pp % p.wid), yy0 = int((pp / p.wid) % p.h);
-      const long long nn = pp / ((long long)p.wid * p.h);
+      // 32-bit division: the host keeps the pixel count below 2^31
+      const uint32_t pp = uint32_t(ok ? pix : pb), t1 = pp / uint32_t(p.wid);
+      const uint32_t nn32 = t1 / uint32_t(p.h);
+      const int xx0 = int(pp - t1 * uint32_t(p.wid)), yy0 = int(t1 - nn32 * uint32_t(p.h));
+      const long long nn = nn32;
       int yy = yy0 + dy_, xx = xx0 + dx_;
       yy += (yy < 0) ? p.h : 0;
       yy -= (yy >= p.h) ? p.h : 0;
@@ -401,6 +403,7 @@ int sp_conv3x3_wgrad(const void* x, const void* dy, float* dw, int n, int h, int
   if (!x || !dy || !dw || n < 1 || h < 1 || w_ < 1 || cin % WM != 0 || cout % 8 != 0)
     return SP_EINVAL;
   const long long npix = (long long)n * h * w_;
+  if (npix >= (1LL << 31)) return SP_EINVAL;  // the kernel's pixel arithmetic is 32-bit
   const unsigned gx = unsigned(9 * (cin / WM)), gy = unsigned((cout + WN - 1) / WN);
   // enough pixel chunks for about four waves of CTAs
   long long want = (long long)sms() * 8 / (gx * gy);
@@ -817,6 +820,7 @@ __global__ void __launch_bounds__(ST_NT) k_conv3x3_strip(const StripParams p, in
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int W2 = p.wid + 2, H2 = p.h + 2;
   const long long HW2 = (long long)W2 * H2, QN = HW2 * p.n;
+  const uint32_t W2u = uint32_t(W2), HW2u = uint32_t(HW2);
   const long long Q0 = (long long)blockIdx.x * ST_M;  // first output position
   const long long S0 = Q0 - (W2 + 1);                 // first strip position
   const int co0 = blockIdx.y * BN;
@@ -854,13 +858,14 @@ __global__ void __launch_bounds__(ST_NT) k_conv3x3_strip(const StripParams p, in
       if (pos < P) {
         off[i] = -1;
         if (q >= 0 && q < QN) {
-          const long long nn = q / HW2, r = q - nn * HW2;
-          int yy = int(r / W2) - 1, xx = int(r % W2) - 1;
+          // 32-bit division (the host keeps every position below 2^31)
+          const uint32_t qu = uint32_t(q), nn = qu / HW2u, r = qu - nn * HW2u, yq = r / W2u;
+          int yy = int(yq) - 1, xx = int(r - yq * W2u) - 1;
           yy += yy < 0 ? p.h : 0;
           yy -= yy >= p.h ? p.h : 0;
           xx += xx < 0 ? p.wid : 0;
           xx -= xx >= p.wid ? p.wid : 0;
-          off[i] = int(((nn * p.h + yy) * p.wid + xx) * p.cin);
+          off[i] = ((int(nn) * p.h + yy) * p.wid + xx) * p.cin;
         }
       }
     }
@@ -901,10 +906,10 @@ __global__ void __launch_bounds__(ST_NT) k_conv3x3_strip(const StripParams p, in
     const int lq = 32 * (warp & 3);
     for (int m = warp >> 2; m < ST_MT; m += 2) {
       const long long q = Q0 + m * 128 + lq + lane;
-      const long long nn = q / HW2, r = q - nn * HW2;
-      const int yp = int(r / W2), xp = int(r % W2);
+      const uint32_t qu = uint32_t(q), nn = qu / HW2u, r = qu - nn * HW2u, yq = r / W2u;
+      const int yp = int(yq), xp = int(r - yq * W2u);
       const bool store = !bad && q < QN && yp >= 1 && yp <= p.h && xp >= 1 && xp <= p.wid;
-      const long long pix = (nn * p.h + (yp - 1)) * p.wid + (xp - 1);
+      const long long pix = ((long long)nn * p.h + (yp - 1)) * p.wid + (xp - 1);
 #pragma unroll
       for (int c16 = 0; c16 < BN / 16; ++c16) {
         uint32_t v[16];
@@ -1028,8 +1033,10 @@ extern "C" int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, cons
     return SP_EINVAL;
   // the epilogue reads the bias 16 channels (64 bytes) at a time
   if (bias && reinterpret_cast<uintptr_t>(bias) % 16 != 0) return SP_EINVAL;
-  // (n (h + 2) + h + 1) (w + 2) + ... stays an int offset per pixel
+  // (n (h + 2) + h + 1) (w + 2) + ... stays an int offset per pixel, and
+  // every padded position (with a strip's reach past the end) below 2^31
   if ((long long)n * h * w_ * cin >= (1LL << 31)) return SP_EINVAL;
+  if ((long long)n * (h + 2) * (w_ + 2) + 4LL * (w_ + 3) + 4096 >= (1LL << 31)) return SP_EINVAL;
   int* err = tc_error_flag();
   if (!err) return SP_ENOMEM;
   const int bn = cout == 32 ? 32 : cout == 64 ? 64 : 128;

@@ -193,6 +193,19 @@ class Model:
         C.check(C.lib().sp_upload_device(self._h, inst, field, ctypes.c_void_p(dev_ptr),
                                          nbytes), self._h)
 
+    def batch_to_device(self, field, dev_ptr, nbytes):
+        """Copy the interiors of every instance to device memory as one dense
+        array [instance][interior, x fastest], one kernel, in the order of the
+        handle's stream (instances of equal extents)."""
+        C.check(C.lib().sp_download_batch_device(self._h, field, ctypes.c_void_p(dev_ptr),
+                                                 nbytes), self._h)
+
+    def batch_from_device(self, field, dev_ptr, nbytes):
+        """Set every instance's interior from one dense device array and
+        refresh all halos, two launches in the order of the handle's stream."""
+        C.check(C.lib().sp_upload_batch_device(self._h, field, ctypes.c_void_p(dev_ptr),
+                                               nbytes), self._h)
+
     def fill_uniform(self, field, seed, lo, hi, inst=0):
         """Seeded SplitMix64 initial values, bit-identical to the oracle."""
         C.check(C.lib().sp_fill_uniform(self._h, inst, field, seed, lo, hi), self._h)

@@ -264,7 +264,12 @@ def seed_fields(m, batch, seed, mean_range=0.4, noise=0.1):
 
 
 def get_batch(m, batch, n, out=None):
+    """The first `batch` instances' fields as [batch, n, n] (one copy kernel
+    when the model holds exactly that many instances)."""
     out = torch.empty(batch, n, n, device="cuda") if out is None else out
+    if m.batch == batch and out.is_contiguous():
+        m.batch_to_device(0, out.data_ptr(), batch * n * n * 4)
+        return out
     for i in range(batch):
         m.field_to_device(0, out[i].data_ptr(), n * n * 4, inst=i)
     return out
@@ -273,6 +278,9 @@ def get_batch(m, batch, n, out=None):
 def put_batch(m, psi):
     n = psi.shape[-1]
     psi = psi.contiguous()
+    if psi.shape[0] == m.batch:
+        m.batch_from_device(0, psi.data_ptr(), psi.numel() * 4)
+        return
     for i in range(psi.shape[0]):
         m.field_from_device(0, psi[i].data_ptr(), n * n * 4, inst=i)
 
@@ -286,7 +294,7 @@ def trajectories(ntraj, nsnap, jump=100, n=256, dt=0.01, seed=1, warm=0):
         m.step(dt, warm)
     snaps = torch.empty(ntraj, nsnap + 1, n, n, device="cuda")
     for s in range(nsnap + 1):
-        get_batch(m, ntraj, n, out=snaps[:, s])
+        snaps[:, s] = get_batch(m, ntraj, n)
         if s < nsnap:
             m.step(dt, jump)
     torch.cuda.synchronize()
@@ -554,6 +562,26 @@ def time_conv(n, side, cin, cout, reps=5):
             "cin": cin, "cout": cout, "ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
 
 
+@torch.no_grad()
+def time_net(batch, n=256, channels=(32, 64, 128, 256), reps=5):
+    """Time one forward pass (a jump) of the network on a batch of random
+    fields: `reps` passes after two warm-up passes, CUDA events."""
+    net = JumpNet(tuple(channels))
+    g = torch.Generator(device="cuda").manual_seed(0)
+    psi = 0.1 * torch.randn(batch, n, n, device="cuda", generator=g)
+    for _ in range(2):
+        net(psi)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        net(psi)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    return {"batch": batch, "n": n, "ms": ms,
+            "tflops": batch * net.flops(n) / (ms * 1e-3) / 1e12}
+
+
 def main(argv=None):
     import argparse
     import json
@@ -561,6 +589,8 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description="train and evaluate the judged k-step jump")
     ap.add_argument("--time-conv", type=int, nargs=4, metavar=("N", "SIDE", "CIN", "COUT"),
                     help="only time one forward convolution layer of this shape and exit")
+    ap.add_argument("--time-net", type=int, default=0, metavar="BATCH",
+                    help="only time one forward pass of the network on this batch and exit")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--ntraj", type=int, default=128, help="training trajectories")
     ap.add_argument("--nsnap", type=int, default=60, help="jumps per trajectory")
@@ -582,6 +612,9 @@ def main(argv=None):
     torch.cuda.set_device(0)
     if a.time_conv:
         print(json.dumps(time_conv(*a.time_conv)))
+        return
+    if a.time_net:
+        print(json.dumps(time_net(a.time_net, a.n, tuple(a.channels))))
         return
     net = JumpNet(tuple(a.channels))
     report = {"params": net.nparams(), "channels": list(a.channels), "n": a.n, "jump": a.jump,
