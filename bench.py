@@ -90,6 +90,9 @@ def parse():
     ap.add_argument("--surrogate-train-steps", type=int, default=6000)
     ap.add_argument("--surrogate-save", default="",
                     help="surrogate: write the trained weights here (torch.save)")
+    ap.add_argument("--surrogate-init", default="",
+                    help="surrogate: start training from these weights")
+    ap.add_argument("--surrogate-lr", type=float, default=1e-3)
     ap.add_argument("--surrogate-jump", type=int, default=2000,
                     help="surrogate: FD steps per learned jump (t_end stays about 6000 steps)")
     ap.add_argument("--surrogate-trajectories", type=int, default=256)
@@ -569,12 +572,16 @@ def run_surrogate(args):
         net.load(torch.load(args.surrogate_load))
         trained = {"weights": os.path.basename(args.surrogate_load)}
     else:
+        if args.surrogate_init:
+            net.load(torch.load(args.surrogate_init))
         t0 = time.perf_counter()
         snaps = S.trajectories(ntraj, nsnap, jump, n, 0.01, seed=1, warm=warm)
-        hist = S.train(net, snaps, args.surrogate_train_steps, 32, 1e-3, log=lambda *_: None)
+        hist = S.train(net, snaps, args.surrogate_train_steps, 32, args.surrogate_lr,
+                       log=lambda *_: None)
         torch.cuda.synchronize()
         trained = {"trajectories": ntraj, "pairs": ntraj * nsnap,
-                   "adam_steps": args.surrogate_train_steps,
+                   "adam_steps": args.surrogate_train_steps, "lr": args.surrogate_lr,
+                   "init": os.path.basename(args.surrogate_init) or None,
                    "train_s": round(time.perf_counter() - t0, 1), "final_loss": hist[-1][1]}
         del snaps
         if args.surrogate_save:

@@ -353,33 +353,30 @@ def train(net, snaps, steps=2000, batch=32, lr=1e-3, seed=0, log_every=200, log=
 # inference: jumps judged by the FD solver
 # ---------------------------------------------------------------------------
 class FdPool:
-    """FD models of 1, 2, 4, ... instances (up to `batch`), on which the
-    intervals of the members the judge rejects are redone: each member of a
-    batch is judged on its own, and only the rejected ones pay for plain FD
-    (padded to the next pool size)."""
+    """FD models of 1, 2, 3, 4, 5, 6, 8, 10, 12, 16, ... instances (about 1.25x
+    apart, up to `batch`), on which the intervals of the members the judge
+    rejects are redone: each member of a batch is judged on its own, and only
+    the rejected ones pay for plain FD (padded to the next pool size)."""
 
     def __init__(self, n, batch, dt):
         self.n, self.dt, self.batch = n, dt, batch
         self.models = {}
+        sizes, s = [], 1
+        while s < batch:
+            sizes.append(s)
+            s = max(s + 1, int(s * 1.25 + 0.5))
+        self.sizes = sizes + [batch]
 
     def get(self, count):
-        size = 1
-        while size < count:
-            size *= 2
-        size = min(size, max(self.batch, count))
+        size = next((s for s in self.sizes if s >= count), count)
         if size not in self.models:
             self.models[size] = fd_model(self.n, size, self.dt)
         return self.models[size], size
 
     def warm(self, steps):
         """Create every size and run `steps` steps on each (graph capture)."""
-        size = 1
-        while True:
-            m, got = self.get(size)
-            m.step(self.dt, steps)
-            if got >= self.batch:
-                break
-            size = got * 2
+        for size in self.sizes:
+            self.get(size)[0].step(self.dt, steps)
 
     def close(self):
         for m in self.models.values():
@@ -608,6 +605,7 @@ def main(argv=None):
     ap.add_argument("--threshold", type=float, default=3.0)
     ap.add_argument("--save", default="", help="write the trained weights here (torch.save)")
     ap.add_argument("--load", default="", help="skip training, load weights")
+    ap.add_argument("--init", default="", help="train starting from these weights")
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
     if a.time_conv:
@@ -622,6 +620,8 @@ def main(argv=None):
     if a.load:
         net.load(torch.load(a.load))
     else:
+        if a.init:
+            net.load(torch.load(a.init))
         t0 = time.perf_counter()
         snaps = trajectories(a.ntraj, a.nsnap, a.jump, a.n, a.dt, seed=1, warm=a.warm)
         report["data_s"] = time.perf_counter() - t0
