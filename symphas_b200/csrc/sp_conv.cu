@@ -17,6 +17,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstdio>
+#include <cstdlib>
+#include <type_traits>
+
 #include "../../include/symphas_b200.h"
 
 namespace sp {
@@ -760,16 +764,20 @@ struct StripParams {
   int S;                     // stages in the ring
 };
 
-constexpr int ST_MT = 4, ST_M = ST_MT * 128, ST_NPROD = 256, ST_NT = ST_NPROD + 32;
+constexpr int ST_NPROD = 256, ST_NT = ST_NPROD + 32;
 constexpr int ST_NPI = 8;  // strip positions per producer thread, at most
 
-template <int BN, int CB>
+// BN output channels x MT 128-position M-tiles per CTA, CB input channels per
+// K block
+template <int BN, int CB, int MT>
 struct StripTile {
   static constexpr int CH = CB / 8;
   static constexpr int B_BYTES = BN * 9 * CB * 2;
-  static constexpr int COLS = ST_MT * BN;  // 128, 256 or 512: powers of two
-  static_assert(COLS == 128 || COLS == 256 || COLS == 512, "tensor memory columns");
+  static constexpr int M = MT * 128;       // output positions per CTA
+  static constexpr int COLS = MT * BN;     // tensor-memory columns: a power of two
+  static_assert(COLS == 64 || COLS == 128 || COLS == 256 || COLS == 512, "tensor memory columns");
   static_assert(CB % 16 == 0 && BN % 16 == 0 && BN <= 128, "tile");
+  static_assert(MT == 2 || MT == 4, "two or four M-tiles: the epilogue's warps take every other one");
 };
 
 // wt, per (output block of BN channels, input block of CB channels), in the
@@ -805,9 +813,10 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
       : "memory");
 }
 
-template <int BN, int CB>
+template <int BN, int CB, int MT>
 __global__ void __launch_bounds__(ST_NT) k_conv3x3_strip(const StripParams p, int* err) {
-  using TT = StripTile<BN, CB>;
+  using TT = StripTile<BN, CB, MT>;
+  constexpr int ST_MT = MT, ST_M = TT::M;
   constexpr int CH = TT::CH;
   extern __shared__ __align__(1024) unsigned char smem[];
   const int S = p.S, P = p.P;
@@ -994,9 +1003,10 @@ __global__ void __launch_bounds__(ST_NT) k_conv3x3_strip(const StripParams p, in
   if (bad) atomicExch(err, 1);
 }
 
-template <int BN, int CB>
-int launch_strip(StripParams p, int* err, cudaStream_t s) {
-  using TT = StripTile<BN, CB>;
+template <int BN, int CB, int MT>
+int launch_strip(StripParams p, int* err, cudaStream_t s, int smax) {
+  using TT = StripTile<BN, CB, MT>;
+  constexpr int ST_M = TT::M;
   const int W2 = p.wid + 2;
   p.P = ((ST_M + 2 * (W2 + 1)) + 7) / 8 * 8;
   if (p.P > ST_NPROD * ST_NPI) return SP_EINVAL;  // rows wider than the producers cover
@@ -1006,18 +1016,21 @@ int launch_strip(StripParams p, int* err, cudaStream_t s) {
   int S = budget / stage;
   if (S < 1) return SP_EINVAL;
   S = S < nk ? S : nk;
-  S = S < 4 ? S : 4;
+  S = S < smax ? S : smax;
   p.S = S;
   int smem = S * stage + (2 * S + 1) * 8 + 16;
-  // 512 tensor-memory columns leave no room for a second CTA on the SM: ask
-  // for enough shared memory that only one is resident
-  if (TT::COLS == 512 && smem < 116 * 1024) smem = 116 * 1024;
+  // no more CTAs on an SM than its 512 tensor-memory columns hold: ask for
+  // enough shared memory (228 KB per SM, 1 KB reserved per CTA) that no
+  // further one is resident
+  const int fit = 512 / TT::COLS;
+  const int floor_smem = 228 * 1024 / (fit + 1) + 1;
+  if (fit < 7 && smem < floor_smem) smem = floor_smem;
   const cudaError_t attr = cudaFuncSetAttribute(
-      k_conv3x3_strip<BN, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      k_conv3x3_strip<BN, CB, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (attr != cudaSuccess) return SP_ECUDA;
   const long long QN = (long long)(p.h + 2) * W2 * p.n;
-  k_conv3x3_strip<BN, CB><<<dim3(unsigned((QN + ST_M - 1) / ST_M), unsigned(p.cout / BN)), ST_NT,
-                            smem, s>>>(p, err);
+  k_conv3x3_strip<BN, CB, MT><<<dim3(unsigned((QN + ST_M - 1) / ST_M), unsigned(p.cout / BN)),
+                                ST_NT, smem, s>>>(p, err);
   return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ECUDA;
 }
 
@@ -1040,7 +1053,18 @@ extern "C" int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, cons
   int* err = tc_error_flag();
   if (!err) return SP_ENOMEM;
   const int bn = cout == 32 ? 32 : cout == 64 ? 64 : 128;
-  const int cb = cin % 32 == 0 && cin <= 64 ? 32 : 16;
+  int cb = cin % 32 == 0 && cin <= 64 ? 32 : 16, mt = 4, smax = 4;
+  // SP_STRIP_SHAPE="mt,cb,stages": M-tiles per CTA (2 or 4), input channels
+  // per K block (16 or 32) and the most ring stages, for timing shapes
+  if (const char* e = getenv("SP_STRIP_SHAPE")) {
+    int a = 0, b = 0, c = 0;
+    if (sscanf(e, "%d,%d,%d", &a, &b, &c) == 3 && (a == 2 || a == 4) && (b == 16 || b == 32) &&
+        c >= 1 && c <= 4 && cin % b == 0) {
+      mt = a;
+      cb = b;
+      smax = c;
+    }
+  }
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   k_tile_weights<<<256, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(w),
                                       static_cast<__nv_bfloat16*>(wt), cin, cout, bn, cb);
@@ -1048,7 +1072,16 @@ extern "C" int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, cons
   StripParams p{static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(wt),
                 bias, static_cast<const __nv_bfloat16*>(res), static_cast<__nv_bfloat16*>(z),
                 static_cast<__nv_bfloat16*>(a), n, h, w_, cin, cout, 0, 0};
-  if (bn == 32) return cb == 32 ? launch_strip<32, 32>(p, err, s) : launch_strip<32, 16>(p, err, s);
-  if (bn == 64) return cb == 32 ? launch_strip<64, 32>(p, err, s) : launch_strip<64, 16>(p, err, s);
-  return cb == 32 ? launch_strip<128, 32>(p, err, s) : launch_strip<128, 16>(p, err, s);
+  auto go = [&](auto bn_c, auto cb_c) {
+    constexpr int BN = decltype(bn_c)::value, CB = decltype(cb_c)::value;
+    return mt == 2 ? launch_strip<BN, CB, 2>(p, err, s, smax)
+                   : launch_strip<BN, CB, 4>(p, err, s, smax);
+  };
+  using I32 = std::integral_constant<int, 32>;
+  using I16 = std::integral_constant<int, 16>;
+  using I64 = std::integral_constant<int, 64>;
+  using I128 = std::integral_constant<int, 128>;
+  if (bn == 32) return cb == 32 ? go(I32{}, I32{}) : go(I32{}, I16{});
+  if (bn == 64) return cb == 32 ? go(I64{}, I32{}) : go(I64{}, I16{});
+  return cb == 32 ? go(I128{}, I32{}) : go(I128{}, I16{});
 }

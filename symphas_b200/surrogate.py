@@ -535,15 +535,18 @@ def evaluate(net, batch=64, jumps=10, jump=100, judge_steps=4, dt=0.01, seed=777
             "fd_ms_per_jump": t_fd / jumps * jump / (jump + judge_steps)}
 
 
-def time_conv(n, side, cin, cout, reps=5):
+def time_conv(n, side, cin, cout, reps=5, inference=False):
     """Time one forward convolution layer of the network's kind (3x3
-    circular, bias, GELU epilogue) on random BF16 data: `reps` launches after
-    two warm-up launches, CUDA events on the current stream."""
+    circular, bias, GELU epilogue writing the pre-activation and the
+    activation, or only the activation with `inference`) on random BF16 data:
+    `reps` launches after two warm-up launches, CUDA events on the current
+    stream."""
     g = torch.Generator().manual_seed(0)
-    x = torch.randn(n, side, side, cin, generator=g).to("cuda", torch.bfloat16)
+    gd = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn(n, side, side, cin, device="cuda", generator=gd).to(torch.bfloat16)
     layer = ConvLayer(cin, cout, g)
-    z = torch.empty(n, side, side, cout, device="cuda", dtype=torch.bfloat16)
-    a = torch.empty_like(z)
+    a = torch.empty(n, side, side, cout, device="cuda", dtype=torch.bfloat16)
+    z = None if inference else torch.empty_like(a)
     scratch = layer.wt
     for _ in range(2):
         _fwd(x, layer.wb, layer.b, None, z, a, cin, cout, scratch)
@@ -588,6 +591,8 @@ def main(argv=None):
                     help="only time one forward convolution layer of this shape and exit")
     ap.add_argument("--time-net", type=int, default=0, metavar="BATCH",
                     help="only time one forward pass of the network on this batch and exit")
+    ap.add_argument("--inference", action="store_true",
+                    help="--time-conv: write only the activation (the network's inference form)")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--ntraj", type=int, default=128, help="training trajectories")
     ap.add_argument("--nsnap", type=int, default=60, help="jumps per trajectory")
@@ -609,7 +614,7 @@ def main(argv=None):
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
     if a.time_conv:
-        print(json.dumps(time_conv(*a.time_conv)))
+        print(json.dumps(time_conv(*a.time_conv, inference=a.inference)))
         return
     if a.time_net:
         print(json.dumps(time_net(a.time_net, a.n, tuple(a.channels))))

@@ -115,10 +115,24 @@ def test_surrogate_network_on_either_kernel(kernel):
     assert rel(d1, d0) < 2e-2
 
 
-@pytest.mark.parametrize("n,h,w,ci,co", [(2, 16, 24, 32, 64), (1, 9, 7, 64, 32),
-                                         (1, 8, 8, 128, 256), (3, 33, 17, 32, 32),
-                                         (1, 10, 10, 16, 128), (2, 64, 64, 64, 128),
-                                         (1, 40, 256, 32, 32), (4, 32, 32, 256, 256)])
+STRIP_SHAPES = [(2, 16, 24, 32, 64), (1, 9, 7, 64, 32), (1, 8, 8, 128, 256), (3, 33, 17, 32, 32),
+                (1, 10, 10, 16, 128), (2, 64, 64, 64, 128), (1, 40, 256, 32, 32),
+                (4, 32, 32, 256, 256)]
+
+
+@pytest.mark.parametrize("tile", ["2,16,1", "2,32,4", "4,16,1", "2,16,4"])
+@pytest.mark.parametrize("n,h,w,ci,co", [STRIP_SHAPES[i] for i in (0, 1, 2, 4, 6)])
+def test_strip_tile_shapes(n, h, w, ci, co, tile, monkeypatch):
+    """Every CTA shape of the strip kernel (SP_STRIP_SHAPE: 2 or 4 M-tiles,
+    16 or 32 input channels per K block, 1 or up to 4 ring stages) gives the
+    convolution: against the reference as the default shape is."""
+    if ci % int(tile.split(",")[1]):
+        pytest.skip("input channels not a multiple of the K block")
+    monkeypatch.setenv("SP_STRIP_SHAPE", tile)
+    test_strip_forward_matches_reference_and_mma_sync(n, h, w, ci, co)
+
+
+@pytest.mark.parametrize("n,h,w,ci,co", STRIP_SHAPES)
 def test_strip_forward_matches_reference_and_mma_sync(n, h, w, ci, co):
     """The gather-once kernel: padded-position strip, taps as operand offsets,
     pre-tiled weights by bulk copy -- ragged position counts, every channel
