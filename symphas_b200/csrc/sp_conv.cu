@@ -1053,7 +1053,23 @@ extern "C" int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, cons
   int* err = tc_error_flag();
   if (!err) return SP_ENOMEM;
   const int bn = cout == 32 ? 32 : cout == 64 ? 64 : 128;
-  int cb = cin % 32 == 0 && cin <= 64 ? 32 : 16, mt = 4, smax = 4;
+  // CTA shape by layer class, from timing every shape on the jump network's
+  // layers (256 samples, 256^2 .. 32^2): narrow outputs gain from more,
+  // smaller CTAs (four or two M-tiles, one stage, so that more CTAs share an
+  // SM and one CTA's gather overlaps another's MMAs and epilogue); wide
+  // inputs and outputs keep the four-stage ring of 32-channel K blocks
+  int cb = 16, mt = 4, smax = 1;
+  if (cout == 64) {
+    mt = 2;
+    cb = cin >= 128 && cin % 32 == 0 ? 32 : 16;
+  } else if (cout >= 128) {
+    if (cin >= 128 && cin % 32 == 0) {
+      cb = 32;
+      smax = 4;
+    } else {
+      mt = 2;
+    }
+  }
   // SP_STRIP_SHAPE="mt,cb,stages": M-tiles per CTA (2 or 4), input channels
   // per K block (16 or 32) and the most ring stages, for timing shapes
   if (const char* e = getenv("SP_STRIP_SHAPE")) {
