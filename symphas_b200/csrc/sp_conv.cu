@@ -1046,6 +1046,8 @@ extern "C" int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, cons
     return SP_EINVAL;
   // the epilogue reads the bias 16 channels (64 bytes) at a time
   if (bias && reinterpret_cast<uintptr_t>(bias) % 16 != 0) return SP_EINVAL;
+  // rows the producers cover with four M-tiles per CTA, whatever shape runs
+  if (w_ > 764) return SP_EINVAL;
   // (n (h + 2) + h + 1) (w + 2) + ... stays an int offset per pixel, and
   // every padded position (with a strip's reach past the end) below 2^31
   if ((long long)n * h * w_ * cin >= (1LL << 31)) return SP_EINVAL;
