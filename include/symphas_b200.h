@@ -268,7 +268,9 @@ int sp_conv_tc_status(int* gave_up);
 /* The same convolution on tcgen05 with every input pixel gathered once: the
  * input staged as a strip of circularly padded positions (one 16-byte row per
  * position and 8-channel chunk), the nine taps as start-address offsets of
- * the MMA operand, four 128-position accumulators per CTA in tensor memory,
+ * the MMA operand, two or four 128-position accumulators per CTA in tensor
+ * memory (the CTA shape is chosen per layer class; SP_STRIP_SHAPE="mt,cb,s"
+ * fixes it for timing),
  * the weights re-tiled into `wt` (9 cin cout bf16 of scratch, device memory)
  * and loaded with one bulk copy per channel block.  cin a multiple of 16,
  * cout 32, 64 or a multiple of 128, w_ <= 764, bias 16-byte aligned; bounded
