@@ -278,6 +278,13 @@ int sp_conv_tc_status(int* gave_up);
 int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, const float* bias,
                          const void* res, void* z, void* a, int n, int h, int w_, int cin,
                          int cout, void* stream);
+/* The same convolution of the nearest 2x up-sampling of x [n][h/2][w_/2][cin]
+ * (h and w_ even: the output's extents), without materialising the
+ * up-sampled input: the strip gather reads each position's source pixel.  No
+ * counterpart in SymPhas (the jump network's decoder). */
+int sp_conv3x3_fwd_strip_up2(const void* x, const void* w, void* wt, const float* bias,
+                             const void* res, void* z, void* a, int n, int h, int w_, int cin,
+                             int cout, void* stream);
 /* dw [cout][3][3][cin] (fp32) += weight gradient of that convolution for the
  * output gradient dy [n][h][w][cout]; cin a multiple of 32, cout of 8, fewer
  * than 2^31 pixels. */

@@ -125,6 +125,9 @@ SIGNATURES = {
     "sp_conv3x3_fwd_strip": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, ctypes.c_int,
                                             ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int, _P]),
+    "sp_conv3x3_fwd_strip_up2": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, ctypes.c_int,
+                                                ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int, _P]),
     "sp_conv_tc_status": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
     "sp_conv3x3_wgrad": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_int, _P]),

@@ -762,6 +762,7 @@ struct StripParams {
   int n, h, wid, cin, cout;
   int P;                     // positions of the strip (multiple of 8)
   int S;                     // stages in the ring
+  int up;                    // 1: x is [N][H/2][W/2][Cin], read nearest-up-sampled
 };
 
 constexpr int ST_NPROD = 256, ST_NT = ST_NPROD + 32;
@@ -874,7 +875,8 @@ __global__ void __launch_bounds__(ST_NT) k_conv3x3_strip(const StripParams p, in
           yy -= yy >= p.h ? p.h : 0;
           xx += xx < 0 ? p.wid : 0;
           xx -= xx >= p.wid ? p.wid : 0;
-          off[i] = ((int(nn) * p.h + yy) * p.wid + xx) * p.cin;
+          off[i] = p.up ? ((int(nn) * (p.h >> 1) + (yy >> 1)) * (p.wid >> 1) + (xx >> 1)) * p.cin
+                        : ((int(nn) * p.h + yy) * p.wid + xx) * p.cin;
         }
       }
     }
@@ -1037,9 +1039,9 @@ int launch_strip(StripParams p, int* err, cudaStream_t s, int smax) {
 }  // namespace conv
 }  // namespace sp
 
-extern "C" int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, const float* bias,
-                                    const void* res, void* z, void* a, int n, int h, int w_,
-                                    int cin, int cout, void* stream) {
+namespace {
+int strip_fwd(const void* x, const void* w, void* wt, const float* bias, const void* res, void* z,
+              void* a, int n, int h, int w_, int cin, int cout, void* stream, int up) {
   using namespace sp::conv;
   if (!x || !w || !wt || (!z && !a) || n < 1 || h < 1 || w_ < 1 || cin % 16 != 0 ||
       !(cout == 32 || cout == 64 || cout % 128 == 0))
@@ -1089,7 +1091,7 @@ extern "C" int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, cons
   if (cudaGetLastError() != cudaSuccess) return SP_ECUDA;
   StripParams p{static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(wt),
                 bias, static_cast<const __nv_bfloat16*>(res), static_cast<__nv_bfloat16*>(z),
-                static_cast<__nv_bfloat16*>(a), n, h, w_, cin, cout, 0, 0};
+                static_cast<__nv_bfloat16*>(a), n, h, w_, cin, cout, 0, 0, up};
   auto go = [&](auto bn_c, auto cb_c) {
     constexpr int BN = decltype(bn_c)::value, CB = decltype(cb_c)::value;
     return mt == 2 ? launch_strip<BN, CB, 2>(p, err, s, smax)
@@ -1102,4 +1104,18 @@ extern "C" int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, cons
   if (bn == 32) return cb == 32 ? go(I32{}, I32{}) : go(I32{}, I16{});
   if (bn == 64) return cb == 32 ? go(I64{}, I32{}) : go(I64{}, I16{});
   return cb == 32 ? go(I128{}, I32{}) : go(I128{}, I16{});
+}
+}  // namespace
+
+extern "C" int sp_conv3x3_fwd_strip(const void* x, const void* w, void* wt, const float* bias,
+                                    const void* res, void* z, void* a, int n, int h, int w_,
+                                    int cin, int cout, void* stream) {
+  return strip_fwd(x, w, wt, bias, res, z, a, n, h, w_, cin, cout, stream, 0);
+}
+
+extern "C" int sp_conv3x3_fwd_strip_up2(const void* x, const void* w, void* wt, const float* bias,
+                                        const void* res, void* z, void* a, int n, int h, int w_,
+                                        int cin, int cout, void* stream) {
+  if (h < 2 || w_ < 2 || h % 2 != 0 || w_ % 2 != 0) return SP_EINVAL;
+  return strip_fwd(x, w, wt, bias, res, z, a, n, h, w_, cin, cout, stream, 1);
 }

@@ -163,6 +163,20 @@ def conv_gelu(x, layer, res=None):
     return a
 
 
+def conv_gelu_up(x, layer, res=None):
+    """conv_gelu(up2(x), layer, res): without autograd, and where the strip
+    kernel runs, one kernel reads the up-sampled input in its gather (no
+    up-sampled copy is made)."""
+    n, h, w, ci = x.shape
+    if torch.is_grad_enabled() or KERNEL != "strip" or not _strip_ok(ci, layer.cout, 2 * w):
+        return conv_gelu(up2(x), layer, res)
+    a = torch.empty(n, 2 * h, 2 * w, layer.cout, device="cuda", dtype=torch.bfloat16)
+    _ok(C.lib().sp_conv3x3_fwd_strip_up2(_p(x.contiguous()), _p(layer.wb), _p(layer.wt),
+                                         _p(layer.b), _p(res), None, _p(a), n, 2 * h, 2 * w, ci,
+                                         layer.cout, _s()), "sp_conv3x3_fwd_strip_up2")
+    return a
+
+
 def pool2(x):
     n, h, w, c = x.shape
     return x.view(n, h // 2, 2, w // 2, 2, c).mean((2, 4))
@@ -214,7 +228,7 @@ class JumpNet:
                 skips.append(x)
                 x = pool2(x)
         for (a, b), s in zip(self.dec, reversed(skips)):
-            x = conv_gelu(up2(x), a, res=s)
+            x = conv_gelu_up(x, a, res=s)
             x = conv_gelu(x, b)
         d = conv(x, self.head)[..., 0].float()
         d = d - d.mean((1, 2), keepdim=True)  # exact mass conservation

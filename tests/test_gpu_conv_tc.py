@@ -175,3 +175,30 @@ def test_strip_forward_rejects_unsupported_shapes():
                                         4, 24, 64, stream()) == C.SP_EINVAL
     assert C.lib().sp_conv3x3_fwd_strip(ptr(x), ptr(wt), ptr(s), None, None, ptr(z), None, 1, 4,
                                         4, 32, 96, stream()) == C.SP_EINVAL
+
+
+@pytest.mark.parametrize("n,h,w,ci,co", [(2, 16, 24, 64, 32), (1, 32, 32, 128, 64),
+                                         (2, 8, 8, 256, 128), (1, 40, 256, 64, 32)])
+def test_strip_up2_equals_strip_on_the_upsampled_input(n, h, w, ci, co):
+    """The decoder's convolution of a 2x nearest up-sampling, with the
+    up-sampling read in the gather: the bits of the strip kernel on the
+    materialised up-sampled input."""
+    torch.manual_seed(2)
+    x = torch.randn(n, h // 2, w // 2, ci, device="cuda").bfloat16()
+    up = x[:, :, None, :, None, :].expand(n, h // 2, 2, w // 2, 2, ci).reshape(n, h, w, ci).contiguous()
+    wt = (torch.randn(co, 3, 3, ci, device="cuda") / (3 * ci ** 0.5)).bfloat16()
+    b = torch.randn(co, device="cuda") * 0.1
+    res = torch.randn(n, h, w, co, device="cuda").bfloat16()
+    scratch = torch.empty(9 * ci * co, device="cuda", dtype=torch.bfloat16)
+    a0 = torch.empty(n, h, w, co, device="cuda", dtype=torch.bfloat16)
+    a1 = torch.full_like(a0, float("nan"))
+    assert C.lib().sp_conv3x3_fwd_strip(ptr(up), ptr(wt), ptr(scratch), ptr(b), ptr(res), None,
+                                        ptr(a0), n, h, w, ci, co, stream()) == C.SP_OK
+    assert C.lib().sp_conv3x3_fwd_strip_up2(ptr(x), ptr(wt), ptr(scratch), ptr(b), ptr(res), None,
+                                            ptr(a1), n, h, w, ci, co, stream()) == C.SP_OK
+    torch.cuda.synchronize()
+    assert status() == 0
+    assert torch.equal(a0, a1)
+    # odd output extents are refused
+    assert C.lib().sp_conv3x3_fwd_strip_up2(ptr(x), ptr(wt), ptr(scratch), ptr(b), ptr(res), None,
+                                            ptr(a1), n, h - 1, w, ci, co, stream()) == C.SP_EINVAL
