@@ -290,6 +290,10 @@ int sp_conv3x3_fwd_strip_up2(const void* x, const void* w, void* wt, const float
  * than 2^31 pixels. */
 int sp_conv3x3_wgrad(const void* x, const void* dy, float* dw, int n, int h, int w_, int cin,
                      int cout, void* stream);
+/* y [n][h/2][w_/2][c] = 2x2 average of x [n][h][w_][c] (bf16, channels last;
+ * h, w_ even, c a multiple of 8, 16-byte aligned rows): the jump network's
+ * pooling at inference.  No counterpart in SymPhas. */
+int sp_avgpool2_bf16(const void* x, void* y, int n, int h, int w_, int c, void* stream);
 /* wf [cin][3][3][cout] = w [cout][3][3][cin] rotated by 180 degrees: the input
  * gradient of the convolution is sp_conv3x3_fwd(dy, wf). */
 int sp_conv3x3_flip(const void* w, void* wf, int cin, int cout, void* stream);

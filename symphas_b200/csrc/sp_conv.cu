@@ -344,6 +344,42 @@ __global__ void __launch_bounds__(WTH) k_conv3x3_wgrad(const WgradParams p) {
 }
 
 // wf[c][t][co] = w[co][8 - t][c]: the forward weights of the data gradient
+// 2x2 average pooling of [N][H][W][C] bf16 (channels last): one thread per
+// output pixel and 8 channels (16 bytes from each of the four inputs), the
+// four values summed in fp32 row by row and scaled by 1/4
+__global__ void k_avgpool2(const __nv_bfloat16* __restrict__ x, __nv_bfloat16* __restrict__ y,
+                           int n, int h, int w, int c, long long total) {
+  const int c8 = c / 8, wo = w / 2, ho = h / 2;
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+       id += (long long)gridDim.x * blockDim.x) {
+    const int cc = int(id % c8);
+    const long long pix = id / c8;
+    const int xo = int(pix % wo);
+    const long long t = pix / wo;
+    const int yo = int(t % ho);
+    const long long nn = t / ho;
+    const long long r0 = ((nn * h + 2 * yo) * w + 2 * xo) * c + cc * 8, r1 = r0 + (long long)w * c;
+    const uint4 a = *reinterpret_cast<const uint4*>(x + r0);
+    const uint4 b = *reinterpret_cast<const uint4*>(x + r0 + c);
+    const uint4 d = *reinterpret_cast<const uint4*>(x + r1);
+    const uint4 e = *reinterpret_cast<const uint4*>(x + r1 + c);
+    const __nv_bfloat162* pa = reinterpret_cast<const __nv_bfloat162*>(&a);
+    const __nv_bfloat162* pb = reinterpret_cast<const __nv_bfloat162*>(&b);
+    const __nv_bfloat162* pd = reinterpret_cast<const __nv_bfloat162*>(&d);
+    const __nv_bfloat162* pe = reinterpret_cast<const __nv_bfloat162*>(&e);
+    __align__(16) __nv_bfloat162 o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float2 fa = __bfloat1622float2(pa[k]), fb = __bfloat1622float2(pb[k]);
+      const float2 fd = __bfloat1622float2(pd[k]), fe = __bfloat1622float2(pe[k]);
+      o[k] = __floats2bfloat162_rn((((fa.x + fb.x) + fd.x) + fe.x) * 0.25f,
+                                   (((fa.y + fb.y) + fd.y) + fe.y) * 0.25f);
+    }
+    *reinterpret_cast<uint4*>(y + ((nn * ho + yo) * wo + xo) * c + cc * 8) =
+        *reinterpret_cast<const uint4*>(o);
+  }
+}
+
 __global__ void k_conv3x3_flip(const __nv_bfloat16* w, __nv_bfloat16* wf, int cin, int cout) {
   const long long total = 9LL * cin * cout;
   for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
@@ -419,6 +455,15 @@ int sp_conv3x3_wgrad(const void* x, const void* dy, float* dw, int n, int h, int
   WgradParams p{static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy), dw,
                 n, h, w_, cin, cout, chunk};
   k_conv3x3_wgrad<<<dim3(gx, gy, gz), WTH, 0, static_cast<cudaStream_t>(stream)>>>(p);
+  return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ECUDA;
+}
+
+int sp_avgpool2_bf16(const void* x, void* y, int n, int h, int w_, int c, void* stream) {
+  if (!x || !y || n < 1 || h < 2 || w_ < 2 || h % 2 || w_ % 2 || c < 8 || c % 8) return SP_EINVAL;
+  const long long total = (long long)n * (h / 2) * (w_ / 2) * (c / 8);
+  const int blocks = int(total / 256 + 1 < 148LL * 16 ? total / 256 + 1 : 148LL * 16);
+  sp::conv::k_avgpool2<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const __nv_bfloat16*>(x), static_cast<__nv_bfloat16*>(y), n, h, w_, c, total);
   return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ECUDA;
 }
 

@@ -202,3 +202,19 @@ def test_strip_up2_equals_strip_on_the_upsampled_input(n, h, w, ci, co):
     # odd output extents are refused
     assert C.lib().sp_conv3x3_fwd_strip_up2(ptr(x), ptr(wt), ptr(scratch), ptr(b), ptr(res), None,
                                             ptr(a1), n, h - 1, w, ci, co, stream()) == C.SP_EINVAL
+
+
+@pytest.mark.parametrize("n,h,w,c", [(3, 16, 24, 32), (1, 256, 256, 64), (2, 8, 4, 256)])
+def test_avgpool2_kernel_matches_torch_mean(n, h, w, c):
+    """The inference pooling kernel: the 2x2 mean of torch within one bf16
+    rounding; odd extents and channel counts that are not a multiple of 8 are
+    refused."""
+    torch.manual_seed(4)
+    x = torch.randn(n, h, w, c, device="cuda").bfloat16()
+    y = torch.full((n, h // 2, w // 2, c), float("nan"), device="cuda", dtype=torch.bfloat16)
+    assert C.lib().sp_avgpool2_bf16(ptr(x), ptr(y), n, h, w, c, stream()) == C.SP_OK
+    torch.cuda.synchronize()
+    want = x.float().view(n, h // 2, 2, w // 2, 2, c).mean((2, 4))
+    assert torch.allclose(y.float(), want, rtol=2.0 ** -7, atol=1e-6)
+    assert C.lib().sp_avgpool2_bf16(ptr(x), ptr(y), n, h - 1, w, c, stream()) == C.SP_EINVAL
+    assert C.lib().sp_avgpool2_bf16(ptr(x), ptr(y), n, h, w, 12, stream()) == C.SP_EINVAL
