@@ -131,6 +131,7 @@ SIGNATURES = {
     "sp_conv_tc_status": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
     "sp_avgpool2_bf16": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, _P]),
+    "sp_embed_channel0_bf16": (ctypes.c_int, [_P, _P, ctypes.c_longlong, ctypes.c_int, _P]),
     "sp_conv3x3_wgrad": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_int, _P]),
     "sp_conv3x3_flip": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, _P]),

@@ -344,6 +344,22 @@ __global__ void __launch_bounds__(WTH) k_conv3x3_wgrad(const WgradParams p) {
 }
 
 // wf[c][t][co] = w[co][8 - t][c]: the forward weights of the data gradient
+// x [pixel][c] = (bf16(psi[pixel]), 0, ..., 0): the network's input channels,
+// one 16-byte store per thread and 8 channels
+__global__ void k_embed0(const float* __restrict__ psi, __nv_bfloat16* __restrict__ x, int c8,
+                         long long total) {
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+       id += (long long)gridDim.x * blockDim.x) {
+    const long long pix = id / c8;
+    const int cc = int(id - pix * c8);
+    __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = __float2bfloat16_rn(0.f);
+    if (cc == 0) v[0] = __float2bfloat16_rn(psi[pix]);
+    *reinterpret_cast<uint4*>(x + id * 8) = *reinterpret_cast<const uint4*>(v);
+  }
+}
+
 // 2x2 average pooling of [N][H][W][C] bf16 (channels last): one thread per
 // output pixel and 8 channels (16 bytes from each of the four inputs), the
 // four values summed in fp32 row by row and scaled by 1/4
@@ -455,6 +471,15 @@ int sp_conv3x3_wgrad(const void* x, const void* dy, float* dw, int n, int h, int
   WgradParams p{static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy), dw,
                 n, h, w_, cin, cout, chunk};
   k_conv3x3_wgrad<<<dim3(gx, gy, gz), WTH, 0, static_cast<cudaStream_t>(stream)>>>(p);
+  return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ECUDA;
+}
+
+int sp_embed_channel0_bf16(const float* psi, void* x, long long npix, int c, void* stream) {
+  if (!psi || !x || npix < 1 || c < 8 || c % 8) return SP_EINVAL;
+  const long long total = npix * (c / 8);
+  const int blocks = int(total / 256 + 1 < 148LL * 16 ? total / 256 + 1 : 148LL * 16);
+  sp::conv::k_embed0<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      psi, static_cast<__nv_bfloat16*>(x), c / 8, total);
   return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ECUDA;
 }
 

@@ -218,3 +218,17 @@ def test_avgpool2_kernel_matches_torch_mean(n, h, w, c):
     assert torch.allclose(y.float(), want, rtol=2.0 ** -7, atol=1e-6)
     assert C.lib().sp_avgpool2_bf16(ptr(x), ptr(y), n, h - 1, w, c, stream()) == C.SP_EINVAL
     assert C.lib().sp_avgpool2_bf16(ptr(x), ptr(y), n, h, w, 12, stream()) == C.SP_EINVAL
+
+
+def test_embed_channel0_kernel():
+    """The network's input: the field in channel 0 (rounded to bf16), zeros
+    elsewhere, as torch builds it."""
+    torch.manual_seed(5)
+    psi = torch.randn(3, 40, 24, device="cuda")
+    x = torch.full((3, 40, 24, 32), float("nan"), device="cuda", dtype=torch.bfloat16)
+    assert C.lib().sp_embed_channel0_bf16(ptr(psi), ptr(x), psi.numel(), 32, stream()) == C.SP_OK
+    torch.cuda.synchronize()
+    want = torch.zeros_like(x)
+    want[..., 0] = psi.bfloat16()
+    assert torch.equal(x, want)
+    assert C.lib().sp_embed_channel0_bf16(ptr(psi), ptr(x), psi.numel(), 12, stream()) == C.SP_EINVAL
