@@ -291,7 +291,8 @@ int sp_conv3x3_fwd_strip_up2(const void* x, const void* w, void* wt, const float
 int sp_conv3x3_wgrad(const void* x, const void* dy, float* dw, int n, int h, int w_, int cin,
                      int cout, void* stream);
 /* x [npix][c] (bf16) = the fp32 field psi [npix] in channel 0 and zeros in
- * the others (c a multiple of 8): the jump network's input in one pass.  No
+ * the others (c a multiple of 8, x 16-byte aligned): the jump network's input
+ * in one pass.  No
  * counterpart in SymPhas. */
 int sp_embed_channel0_bf16(const float* psi, void* x, long long npix, int c, void* stream);
 /* y [n][h/2][w_/2][c] = 2x2 average of x [n][h][w_][c] (bf16, channels last;

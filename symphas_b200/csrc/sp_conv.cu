@@ -476,6 +476,7 @@ int sp_conv3x3_wgrad(const void* x, const void* dy, float* dw, int n, int h, int
 
 int sp_embed_channel0_bf16(const float* psi, void* x, long long npix, int c, void* stream) {
   if (!psi || !x || npix < 1 || c < 8 || c % 8) return SP_EINVAL;
+  if (reinterpret_cast<uintptr_t>(x) % 16 != 0) return SP_EINVAL;  // 16-byte stores
   const long long total = npix * (c / 8);
   const int blocks = int(total / 256 + 1 < 148LL * 16 ? total / 256 + 1 : 148LL * 16);
   sp::conv::k_embed0<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
@@ -485,6 +486,8 @@ int sp_embed_channel0_bf16(const float* psi, void* x, long long npix, int c, voi
 
 int sp_avgpool2_bf16(const void* x, void* y, int n, int h, int w_, int c, void* stream) {
   if (!x || !y || n < 1 || h < 2 || w_ < 2 || h % 2 || w_ % 2 || c < 8 || c % 8) return SP_EINVAL;
+  if (reinterpret_cast<uintptr_t>(x) % 16 != 0 || reinterpret_cast<uintptr_t>(y) % 16 != 0)
+    return SP_EINVAL;  // 16-byte loads and stores
   const long long total = (long long)n * (h / 2) * (w_ / 2) * (c / 8);
   const int blocks = int(total / 256 + 1 < 148LL * 16 ? total / 256 + 1 : 148LL * 16);
   sp::conv::k_avgpool2<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
